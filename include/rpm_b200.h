@@ -1,0 +1,149 @@
+/*
+ * rpm_b200.h -- C ABI of librpm_b200.so, the B200 (sm_100a) engine for the
+ * radical-pair hot path of sam-not-smart/RPM.
+ *
+ * Reference files are cited relative to "Realistic system size/code/":
+ *   ENG  = rpm_statevector_engine.py
+ *   CORE = poster_reproduction/core.py
+ *   JD   = rpm_quantum_needle_jd_sweeps.py
+ *
+ * Conventions
+ *   - Every function returns an int status: RPM_OK (0) or one of RPM_E_*.
+ *     rpm_last_error() returns a thread-local message for the last failure.
+ *     No C++ exception crosses this boundary.
+ *   - Complex numbers are interleaved (re, im): complex128 = 2 x double,
+ *     complex64 = 2 x float.  State vectors are C-order over the tensor
+ *     dimensions (the first axis slowest), as NumPy's reshape(dims).
+ *   - Pointers named *_dev are device pointers owned by the caller (e.g.
+ *     torch tensors); *_host are host pointers.  `stream` is a cudaStream_t
+ *     (NULL = legacy default stream).  Calls on one rpm_system are not
+ *     re-entrant: the system owns internal scratch buffers.
+ */
+#ifndef RPM_B200_H
+#define RPM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RPM_OK 0
+#define RPM_E_INVALID 1      /* bad argument; the host raises ValueError      */
+#define RPM_E_CUDA 2         /* CUDA runtime failure                          */
+#define RPM_E_NOMEM 3        /* device or host allocation failed              */
+#define RPM_E_UNSUPPORTED 4  /* size or shape outside the compiled limits     */
+#define RPM_E_NOT_HERMITIAN 5 /* a local term fails the Hermiticity check     */
+#define RPM_E_NUMERIC 6      /* eigen-solver did not converge / non-finite    */
+#define RPM_E_TIMEOUT 7      /* a bounded device wait gave up                 */
+
+#define RPM_MAX_AXES 32      /* tensor axes of one system                     */
+#define RPM_MAX_TERM_AXES 4  /* axes one local term may act on                */
+#define RPM_MAX_LOCAL_DIM 64 /* local operator side                           */
+#define RPM_MAX_KRYLOV 128   /* Krylov dimension                              */
+
+#define RPM_PREC_C64 64      /* complex64 state arithmetic (FP32)             */
+#define RPM_PREC_C128 128    /* complex128 state arithmetic (FP64)            */
+
+typedef struct rpm_system rpm_system;
+
+/* One local term: `naxes` distinct tensor axes and a row-major complex128
+ * operator of side prod(dims[axes]) -- ENG:28-34 (LocalTerm). */
+typedef struct rpm_term {
+  int naxes;
+  int axes[RPM_MAX_TERM_AXES];
+  const double* op;
+} rpm_term;
+
+const char* rpm_last_error(void);
+int rpm_version(void);
+/* Number of CUDA devices visible; 0 when no driver or device. */
+int rpm_device_count(int* count);
+
+/* Build a Hamiltonian system.  Replaces ENG:46-93 (MatrixFreeHamiltonian.__init__,
+ * _compile_term: axis/shape/Hermiticity checks with `hermitian_tolerance`) and,
+ * when nleft > 0, ENG:142-219 (CompiledFullPairHamiltonian.__init__: radical
+ * split into left/right CSR blocks and the 4x4 electron-pair operator; the
+ * first left and first right axis are the electron pair).  With nleft == 0
+ * the generic per-term kernel is used.  host_only != 0 builds the host tables
+ * without touching the GPU (for inspection). */
+int rpm_system_create(const int* dims, int ndims, const rpm_term* terms, int nterms,
+                      const int* left_axes, int nleft, const int* right_axes, int nright,
+                      double hermitian_tolerance, int host_only, rpm_system** out);
+int rpm_system_destroy(rpm_system* sys);
+/* dimension N, split flag, left/right group sizes and CSR nonzero counts. */
+int rpm_system_info(const rpm_system* sys, long long* dimension, int* split,
+                    int* nl, int* nr, int* nnz_left, int* nnz_right);
+/* Copy the host CSR tables of a split system (arrays sized from rpm_system_info):
+ * row pointers (n+1), columns, complex128 values, memory offsets of each
+ * left/right group index, and the 4x4 pair operator (16 complex128). */
+int rpm_system_split_tables(const rpm_system* sys, int* lptr, int* lcol, double* lval,
+                            int* rptr, int* rcol, double* rval, long long* offl,
+                            long long* offr, double* pair);
+
+/* out = H psi for `batch` vectors spaced `ld` elements apart.
+ * Replaces ENG:95-108 (MatrixFreeHamiltonian.matvec), ENG:110-114 (matmat)
+ * and ENG:221-253 (CompiledFullPairHamiltonian.matvec/matmat). */
+int rpm_hpsi(rpm_system* sys, int precision, const void* psi_dev, void* out_dev,
+             int batch, long long ld, void* stream);
+
+/* FP64 Hermitian Lanczos with two classical Gram-Schmidt passes, replacing
+ * ENG:651-688 (AdaptiveLanczosPropagator._basis).  basis_dev holds max_dim
+ * complex128 columns of length N (column j at basis_dev + j*N); alpha_dev
+ * (max_dim) and beta_dev (max_dim-1) receive the tridiagonal.  On return
+ * *actual_host is the basis size (smaller than max_dim after a breakdown
+ * with beta <= breakdown_tol) and *norm_host = ||state||.  Raises
+ * RPM_E_INVALID for the zero vector (ENG:656-658).  Synchronises `stream`. */
+int rpm_lanczos_basis(rpm_system* sys, const void* state_dev, int max_dim,
+                      double breakdown_tol, void* basis_dev, double* alpha_dev,
+                      double* beta_dev, int* actual_host, double* norm_host, void* stream);
+
+/* Spectral data of the leading d x d block of the tridiagonal (alpha, beta)
+ * for each of `ndims` sizes: eigenvalues and eigenvectors by implicit QR with
+ * Wilkinson shifts in FP64 (replaces scipy.linalg.eigh_tridiagonal in
+ * ENG:569-609).  spectra_dev holds ndims records of RPM_SPECTRUM_DOUBLES. */
+#define RPM_SPECTRUM_DOUBLES (RPM_MAX_KRYLOV + RPM_MAX_KRYLOV * RPM_MAX_KRYLOV + 2)
+int rpm_tridiag_spectra(const double* alpha_dev, const double* beta_dev, int ndims,
+                        const int* dims_host, double* spectra_dev, void* stream);
+
+/* One evaluation request against spectra records: coefficients
+ * c = exp(-i T_hi t) e1, the embedded error
+ * safety*state_norm*||c - [c_lo; 0]|| (ENG:690-715, 876-888; lo < 0: zero)
+ * and, when gram_dev != NULL, state_norm^2 c^H G c (ENG:532-538). */
+typedef struct rpm_krylov_req {
+  int hi;       /* spectra record of the propagating dimension */
+  int lo;       /* spectra record of the embedded dimension, or -1 */
+  double time;  /* time offset in us */
+} rpm_krylov_req;
+int rpm_krylov_eval(const double* spectra_dev, int nreq, const rpm_krylov_req* reqs_host,
+                    double safety, double state_norm, const void* gram_dev, int gram_ld,
+                    void* coef_dev, int coef_ld, double* err_host, double* value_host,
+                    void* stream);
+
+/* G = A^H A for the singlet amplitudes A = (V[0,1,:] - V[1,0,:])/sqrt 2 of the
+ * first m complex128 basis columns (ENG:521-529); gram_dev is m x m complex128,
+ * Hermitian-symmetrised. */
+int rpm_singlet_gram(rpm_system* sys, const void* basis_dev, int m, void* gram_dev, void* stream);
+
+/* out = scale * V[:, :m] c (complex128), and *norm_host = ||out|| when
+ * norm_host != NULL (ENG:895, 904, 909).  Synchronises when norm_host != NULL. */
+int rpm_combine(rpm_system* sys, const void* basis_dev, int m, const void* coef_dev,
+                double scale, void* out_dev, double* norm_host, void* stream);
+
+/* Singlet population ||(psi[0,1,:] - psi[1,0,:])/sqrt2||^2 of `batch`
+ * complex128 vectors of length n (n divisible by 4, electrons first) spaced
+ * `ld` apart (ENG:492-497) into values_host.  Synchronises. */
+int rpm_singlet_population(const void* psi_dev, long long n, int batch, long long ld,
+                           double* values_host, void* stream);
+
+/* ||psi|| (complex128) into *norm_host.  Synchronises. */
+int rpm_norm(rpm_system* sys, const void* psi_dev, double* norm_host, void* stream);
+
+/* Composite Simpson yield  sum_k w_k exp(-t_k/tau) P_k / tau  in FP64 with
+ * compensated summation, for `batch` population rows of length n spaced
+ * `ld` apart (JD:418-420, scipy.integrate.simpson odd/even rules). */
+int rpm_simpson_yield(const double* times_dev, const double* pops_dev, int n, int batch,
+                      long long ld, double lifetime_us, double* yields_dev, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RPM_B200_H */

@@ -1,0 +1,699 @@
+// FP64 Krylov machinery for the plain (single-vector, complex128) propagator.
+//
+//   * Hermitian Lanczos with two classical Gram-Schmidt passes
+//     (rpm_statevector_engine.py:651-688), as a fixed launch sequence per
+//     basis vector with device-side breakdown flag, so no host round trip
+//     happens inside a basis build.
+//   * Deterministic reductions: every block writes its partial sums, the
+//     last block to finish (atomic ticket) adds them in block order.
+//   * Symmetric tridiagonal eigen-decomposition by implicit QR with Wilkinson
+//     shifts (Golub & Van Loan, Matrix Computations, sec. 8.3): one thread runs
+//     the scalar bulge chase and records the Givens rotations; all threads
+//     then apply them to their own rows of the eigenvector matrix.
+//   * exp(-i T t) e1 coefficients, embedded error norms and projected singlet
+//     populations (rpm_statevector_engine.py:569-609, 690-715, 521-538).
+//   * Singlet Gram, state recombination, norms and the Simpson yield
+//     (rpm_quantum_needle_jd_sweeps.py:418-420).
+#include <cfloat>
+#include <cmath>
+
+#include "common.cuh"
+#include "krylov.cuh"
+
+namespace rpm {
+
+constexpr int kThreads = 256;
+constexpr int kRowsPerThread = 4;
+constexpr int kRowsPerBlock = kThreads * kRowsPerThread;
+
+// ---------------------------------------------------------------------------
+// Lanczos kernels (single vector, complex128)
+// Device scalars (LanczosScalars) live in SLOT_SMALL.
+// ---------------------------------------------------------------------------
+struct LanczosScalars {
+  unsigned counter[8];
+  int stop;       // basis size after a breakdown (0 = running)
+  int pad;
+  double norm;    // ||state||
+  double2 h1[RPM_MAX_KRYLOV];
+  double2 h2[RPM_MAX_KRYLOV];
+};
+
+// v0 = state / ||state|| ; first launch computes ||state||^2 partials.
+__global__ void __launch_bounds__(kThreads) k_norm_partial(const double2* __restrict__ x, long long n,
+                                                          double2* partials, LanczosScalars* sc, int init) {
+  __shared__ double2 scratch[32];
+  __shared__ double2 tot[1];
+  double2 acc[1] = {make_double2(0.0, 0.0)};
+  const long long base = (long long)blockIdx.x * kRowsPerBlock + threadIdx.x;
+#pragma unroll
+  for (int r = 0; r < kRowsPerThread; ++r) {
+    const long long i = base + (long long)r * kThreads;
+    if (i < n) {
+      const double2 v = x[i];
+      acc[0].x = fma(v.x, v.x, fma(v.y, v.y, acc[0].x));
+    }
+  }
+  block_sum2<1>(acc, scratch, tot);
+  if (threadIdx.x == 0) partials[blockIdx.x] = tot[0];
+  if (last_block(&sc->counter[0])) {
+    __shared__ double2 res[1];
+    finish_sums(partials, gridDim.x, 1, res);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      sc->norm = sqrt(res[0].x);
+      if (init) sc->stop = 0;
+      if (init && !(sc->norm > 0.0)) sc->stop = -1;
+      sc->counter[0] = 0;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_scale_to(const double2* __restrict__ x, double2* __restrict__ y,
+                                                      long long n, const LanczosScalars* sc) {
+  if (sc->stop != 0) return;
+  const double inv = 1.0 / sc->norm;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double2 v = x[i];
+    y[i] = make_double2(v.x * inv, v.y * inv);
+  }
+}
+
+// alpha_j = Re <v_j, w>
+__global__ void __launch_bounds__(kThreads) k_alpha(const double2* __restrict__ v, const double2* __restrict__ w,
+                                                   long long n, double2* partials, LanczosScalars* sc, double* alpha,
+                                                   int j) {
+  if (sc->stop != 0) return;
+  __shared__ double2 scratch[32];
+  __shared__ double2 tot[1];
+  double2 acc[1] = {make_double2(0.0, 0.0)};
+  const long long base = (long long)blockIdx.x * kRowsPerBlock + threadIdx.x;
+#pragma unroll
+  for (int r = 0; r < kRowsPerThread; ++r) {
+    const long long i = base + (long long)r * kThreads;
+    if (i < n) acc[0] = cfma_conj(v[i], w[i], acc[0]);
+  }
+  block_sum2<1>(acc, scratch, tot);
+  if (threadIdx.x == 0) partials[blockIdx.x] = tot[0];
+  if (last_block(&sc->counter[1])) {
+    __shared__ double2 res[1];
+    finish_sums(partials, gridDim.x, 1, res);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      alpha[j] = res[0].x;
+      sc->counter[1] = 0;
+    }
+  }
+}
+
+// Block dot products  h[k] = <V_k, w>  for k < count over this block's rows,
+// with w held in registers.  Results into partials[k * nblocks + block].
+__device__ void block_dots(const double2* __restrict__ basis, long long n, int count, const double2 (&w)[kRowsPerThread],
+                           double2* partials) {
+  __shared__ double2 scratch[32 * 8];
+  __shared__ double2 tot[8];
+  const long long base = (long long)blockIdx.x * kRowsPerBlock + threadIdx.x;
+  for (int k0 = 0; k0 < count; k0 += 8) {
+    double2 acc[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) acc[c] = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      if (k0 + c < count) {
+        const double2* vk = basis + (size_t)(k0 + c) * n;
+#pragma unroll
+        for (int r = 0; r < kRowsPerThread; ++r) {
+          const long long i = base + (long long)r * kThreads;
+          if (i < n) acc[c] = cfma_conj(vk[i], w[r], acc[c]);
+        }
+      }
+    }
+    block_sum2<8>(acc, scratch, tot);
+    if (threadIdx.x < 8 && k0 + threadIdx.x < count) partials[(size_t)(k0 + threadIdx.x) * gridDim.x + blockIdx.x] = tot[threadIdx.x];
+  }
+}
+
+// w <- w - alpha_j v_j - beta_{j-1} v_{j-1};  h1 = V[:, :j+1]^H w
+__global__ void __launch_bounds__(kThreads) k_update_dots(const double2* __restrict__ basis, double2* __restrict__ w,
+                                                         long long n, int j, const double* alpha, const double* beta,
+                                                         double2* partials, LanczosScalars* sc) {
+  if (sc->stop != 0) return;
+  const double a = alpha[j];
+  const double b = j > 0 ? beta[j - 1] : 0.0;
+  const double2* vj = basis + (size_t)j * n;
+  const double2* vp = basis + (size_t)(j > 0 ? j - 1 : 0) * n;
+  double2 wr[kRowsPerThread];
+  const long long base = (long long)blockIdx.x * kRowsPerBlock + threadIdx.x;
+#pragma unroll
+  for (int r = 0; r < kRowsPerThread; ++r) {
+    const long long i = base + (long long)r * kThreads;
+    wr[r] = make_double2(0.0, 0.0);
+    if (i < n) {
+      double2 x = w[i];
+      const double2 v = vj[i];
+      x.x -= a * v.x;
+      x.y -= a * v.y;
+      if (j > 0) {
+        const double2 u = vp[i];
+        x.x -= b * u.x;
+        x.y -= b * u.y;
+      }
+      wr[r] = x;
+      w[i] = x;
+    }
+  }
+  block_dots(basis, n, j + 1, wr, partials);
+  if (last_block(&sc->counter[2])) {
+    finish_sums(partials, gridDim.x, j + 1, sc->h1);
+    __syncthreads();
+    if (threadIdx.x == 0) sc->counter[2] = 0;
+  }
+}
+
+// w <- w - V h ; then (second == 1) h2 = V^H w, or (second == 0) ||w||^2 -> beta_j
+__global__ void __launch_bounds__(kThreads) k_axpy_then(const double2* __restrict__ basis, double2* __restrict__ w,
+                                                       long long n, int j, int second, int last, double tol,
+                                                       double* beta, double2* partials, LanczosScalars* sc) {
+  if (sc->stop != 0) return;
+  __shared__ double2 h[RPM_MAX_KRYLOV];
+  const double2* hsrc = second ? sc->h1 : sc->h2;
+  for (int k = threadIdx.x; k <= j; k += blockDim.x) h[k] = hsrc[k];
+  __syncthreads();
+  double2 wr[kRowsPerThread];
+  const long long base = (long long)blockIdx.x * kRowsPerBlock + threadIdx.x;
+#pragma unroll
+  for (int r = 0; r < kRowsPerThread; ++r) {
+    const long long i = base + (long long)r * kThreads;
+    wr[r] = make_double2(0.0, 0.0);
+    if (i < n) {
+      // CGS: w - V h accumulated as one product, then subtracted
+      double2 vh = make_double2(0.0, 0.0);
+      for (int k = 0; k <= j; ++k) vh = cfma(basis[(size_t)k * n + i], h[k], vh);
+      double2 x = w[i];
+      x.x -= vh.x;
+      x.y -= vh.y;
+      wr[r] = x;
+      w[i] = x;
+    }
+  }
+  if (second) {
+    block_dots(basis, n, j + 1, wr, partials);
+    if (last_block(&sc->counter[3])) {
+      finish_sums(partials, gridDim.x, j + 1, sc->h2);
+      __syncthreads();
+      if (threadIdx.x == 0) sc->counter[3] = 0;
+    }
+    return;
+  }
+  if (last) return;
+  __shared__ double2 scratch[32];
+  __shared__ double2 tot[1];
+  double2 acc[1] = {make_double2(0.0, 0.0)};
+#pragma unroll
+  for (int r = 0; r < kRowsPerThread; ++r) acc[0].x = fma(wr[r].x, wr[r].x, fma(wr[r].y, wr[r].y, acc[0].x));
+  block_sum2<1>(acc, scratch, tot);
+  if (threadIdx.x == 0) partials[blockIdx.x] = tot[0];
+  if (last_block(&sc->counter[4])) {
+    __shared__ double2 res[1];
+    finish_sums(partials, gridDim.x, 1, res);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const double bj = sqrt(res[0].x);
+      beta[j] = bj;
+      if (bj <= tol) sc->stop = j + 1;
+      sc->counter[4] = 0;
+    }
+  }
+}
+
+// v_{j+1} = w / beta_j
+__global__ void __launch_bounds__(kThreads) k_next_vector(const double2* __restrict__ w, double2* __restrict__ next,
+                                                         long long n, const double* beta, int j,
+                                                         const LanczosScalars* sc) {
+  if (sc->stop != 0) return;
+  const double inv = 1.0 / beta[j];
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double2 v = w[i];
+    next[i] = make_double2(v.x * inv, v.y * inv);
+  }
+}
+
+// spectra record layout (doubles): [0] size, [1] status, [2 .. 2+MAXK) eigenvalues,
+// then MAXK x MAXK eigenvectors (row i = component i).
+__global__ void k_tridiag_spectra(const double* __restrict__ alpha, const double* __restrict__ beta, const int* dims,
+                                  double* spectra) {
+  extern __shared__ double sm[];
+  double* z = sm;                                  // m * m
+  double* d = z + RPM_MAX_KRYLOV * RPM_MAX_KRYLOV;  // m
+  double* e = d + RPM_MAX_KRYLOV;                  // m
+  double2* rot = reinterpret_cast<double2*>(e + RPM_MAX_KRYLOV);
+  const int m = dims[blockIdx.x];
+  double* rec = spectra + (size_t)blockIdx.x * RPM_SPECTRUM_DOUBLES;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    d[i] = alpha[i];
+    e[i] = (i + 1 < m) ? beta[i] : 0.0;
+  }
+  __syncthreads();
+  const int status = tridiag_qr(m, d, e, z, m, rot);
+  for (int i = threadIdx.x; i < m; i += blockDim.x) rec[2 + i] = d[i];
+  for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
+    const int i = idx / m, k = idx % m;
+    rec[2 + RPM_MAX_KRYLOV + i * RPM_MAX_KRYLOV + k] = z[i * m + k];
+  }
+  if (threadIdx.x == 0) {
+    rec[0] = m;
+    rec[1] = status;
+  }
+}
+
+__global__ void k_krylov_eval(const double* __restrict__ spectra, const rpm_krylov_req* reqs, double safety,
+                              double state_norm, const double2* __restrict__ gram, int gram_ld, double2* coef,
+                              int coef_ld, double* err_out, double* value_out) {
+  __shared__ double2 ph[RPM_MAX_KRYLOV], chi[RPM_MAX_KRYLOV], clo[RPM_MAX_KRYLOV];
+  __shared__ double red[kThreads / 32];
+  const rpm_krylov_req rq = reqs[blockIdx.x];
+  const double* rhi = spectra + (size_t)rq.hi * RPM_SPECTRUM_DOUBLES;
+  const int mh = (int)rhi[0];
+  spectral_coefficients(rhi, rq.time, ph, chi);
+  int ml = 0;
+  if (rq.lo >= 0) {
+    const double* rlo = spectra + (size_t)rq.lo * RPM_SPECTRUM_DOUBLES;
+    ml = (int)rlo[0];
+    spectral_coefficients(rlo, rq.time, ph, clo);
+  }
+  for (int i = threadIdx.x; i < mh; i += blockDim.x) coef[(size_t)blockIdx.x * coef_ld + i] = chi[i];
+  // ||c_hi - [c_lo; 0]||
+  double acc = 0.0;
+  if (rq.lo >= 0) {
+    for (int i = threadIdx.x; i < mh; i += blockDim.x) {
+      double2 dlt = chi[i];
+      if (i < ml) {
+        dlt.x -= clo[i].x;
+        dlt.y -= clo[i].y;
+      }
+      acc = fma(dlt.x, dlt.x, fma(dlt.y, dlt.y, acc));
+    }
+  }
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    err_out[blockIdx.x] = rq.lo >= 0 ? safety * state_norm * sqrt(s) : 0.0;
+  }
+  __syncthreads();
+  if (gram) {
+    // c^H G c
+    double v = 0.0;
+    for (int i = threadIdx.x; i < mh; i += blockDim.x) {
+      double2 gc = make_double2(0.0, 0.0);
+      for (int k = 0; k < mh; ++k) gc = cfma(gram[(size_t)i * gram_ld + k], chi[k], gc);
+      v += chi[i].x * gc.x + chi[i].y * gc.y;
+    }
+    v = warp_sum(v);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+      value_out[blockIdx.x] = state_norm * state_norm * s;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Singlet Gram  G = A^H A,  A[:, k] = (V_k[M:2M] - V_k[2M:3M]) / sqrt 2
+// ---------------------------------------------------------------------------
+constexpr int kGramRows = 32;
+
+__global__ void __launch_bounds__(kThreads) k_gram_partial(const double2* __restrict__ basis, long long n, int m,
+                                                          double2* partials) {
+  extern __shared__ double2 a[];  // kGramRows x m
+  const long long quarter = n / 4;
+  const double rs2 = 0.70710678118654752440;
+  const int pairs = m * m;
+  double2 acc[16];
+  const int per = (pairs + blockDim.x - 1) / blockDim.x;  // <= 16 for m <= 64
+#pragma unroll
+  for (int q = 0; q < 16; ++q) acc[q] = make_double2(0.0, 0.0);
+  for (long long r0 = (long long)blockIdx.x * kGramRows; r0 < quarter; r0 += (long long)gridDim.x * kGramRows) {
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kGramRows * m; idx += blockDim.x) {
+      const int rr = idx / m, k = idx % m;
+      const long long i = r0 + rr;
+      double2 v = make_double2(0.0, 0.0);
+      if (i < quarter) {
+        const double2 p = basis[(size_t)k * n + quarter + i];
+        const double2 q = basis[(size_t)k * n + 2 * quarter + i];
+        v = make_double2((p.x - q.x) * rs2, (p.y - q.y) * rs2);
+      }
+      a[rr * m + k] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int pr = threadIdx.x + q * blockDim.x;
+      if (q < per && pr < pairs) {
+        const int k = pr / m, l = pr % m;
+        double2 s = acc[q];
+        for (int rr = 0; rr < kGramRows; ++rr) s = cfma_conj(a[rr * m + k], a[rr * m + l], s);
+        acc[q] = s;
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const int pr = threadIdx.x + q * blockDim.x;
+    if (q < per && pr < pairs) partials[(size_t)pr * gridDim.x + blockIdx.x] = acc[q];
+  }
+}
+
+__global__ void k_gram_finish(const double2* __restrict__ partials, int nblocks, int m, double2* gram) {
+  const int pr = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pr >= m * m) return;
+  const int k = pr / m, l = pr % m;
+  double2 s = make_double2(0.0, 0.0), t = make_double2(0.0, 0.0);
+  for (int b = 0; b < nblocks; ++b) {
+    s = cadd(s, partials[(size_t)(k * m + l) * nblocks + b]);
+    t = cadd(t, partials[(size_t)(l * m + k) * nblocks + b]);
+  }
+  // Hermitian symmetrisation 0.5 (G + G^H)
+  gram[(size_t)k * m + l] = make_double2(0.5 * (s.x + t.x), 0.5 * (s.y - t.y));
+}
+
+// ---------------------------------------------------------------------------
+// out = scale * V c  (+ ||out||^2)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_combine(const double2* __restrict__ basis, long long n, int m,
+                                                     const double2* __restrict__ coef, double scale,
+                                                     double2* __restrict__ out, double2* partials, unsigned* counter,
+                                                     double* norm_out) {
+  __shared__ double2 c[RPM_MAX_KRYLOV];
+  __shared__ double2 scratch[32];
+  __shared__ double2 tot[1];
+  for (int k = threadIdx.x; k < m; k += blockDim.x) c[k] = coef[k];
+  __syncthreads();
+  double2 acc[1] = {make_double2(0.0, 0.0)};
+  const long long base = (long long)blockIdx.x * kRowsPerBlock + threadIdx.x;
+#pragma unroll
+  for (int r = 0; r < kRowsPerThread; ++r) {
+    const long long i = base + (long long)r * kThreads;
+    if (i < n) {
+      double2 s = make_double2(0.0, 0.0);
+      for (int k = 0; k < m; ++k) s = cfma(basis[(size_t)k * n + i], c[k], s);
+      s.x *= scale;
+      s.y *= scale;
+      out[i] = s;
+      acc[0].x = fma(s.x, s.x, fma(s.y, s.y, acc[0].x));
+    }
+  }
+  block_sum2<1>(acc, scratch, tot);
+  if (threadIdx.x == 0) partials[blockIdx.x] = tot[0];
+  if (last_block(counter)) {
+    __shared__ double2 res[1];
+    finish_sums(partials, gridDim.x, 1, res);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      *norm_out = sqrt(res[0].x);
+      *counter = 0;
+    }
+  }
+}
+
+// Per-vector reductions over a batch: kind 0 = ||x||^2, kind 1 = singlet population.
+__global__ void __launch_bounds__(kThreads) k_batch_reduce(const double2* __restrict__ x, long long n, long long ld,
+                                                          int kind, double* out) {
+  __shared__ double red[kThreads / 32];
+  const double2* v = x + (long long)blockIdx.x * ld;
+  double acc = 0.0;
+  if (kind == 0) {
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) acc = fma(v[i].x, v[i].x, fma(v[i].y, v[i].y, acc));
+  } else {
+    const long long q = n / 4;
+    for (long long i = threadIdx.x; i < q; i += blockDim.x) {
+      const double2 a = v[q + i], b = v[2 * q + i];
+      const double re = a.x - b.x, im = a.y - b.y;
+      acc = fma(re, re, fma(im, im, acc));
+    }
+    acc *= 0.5;
+  }
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    out[blockIdx.x] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Simpson yield with Neumaier-compensated FP64 sums (one block per row)
+// ---------------------------------------------------------------------------
+struct Kahan {
+  double s, c;
+  __device__ void add(double v) {
+    const double t = s + v;
+    c += (fabs(s) >= fabs(v)) ? ((s - t) + v) : ((v - t) + s);
+    s = t;
+  }
+};
+
+__device__ __forceinline__ double simpson_integrand(const double* t, const double* p, int k, double tau) {
+  return exp(-t[k] / tau) * p[k] / tau;
+}
+
+__global__ void k_simpson(const double* __restrict__ t, const double* __restrict__ pops, int n, long long ld,
+                          double tau, double* out) {
+  __shared__ double ss[kThreads], cs[kThreads];
+  const double* p = pops + (long long)blockIdx.x * ld;
+  Kahan acc{0.0, 0.0};
+  // panels over [0, stop]: odd n -> stop = n - 1, even n -> stop = n - 2 (end correction below)
+  const int stop = (n % 2 == 1) ? n - 1 : n - 2;
+  if (n >= 3) {
+    for (int k = 2 * threadIdx.x; k + 2 <= stop; k += 2 * blockDim.x) {
+      const double h0 = t[k + 1] - t[k], h1 = t[k + 2] - t[k + 1];
+      const double hs = h0 + h1, hp = h0 * h1, r = h0 / h1;
+      const double f0 = simpson_integrand(t, p, k, tau), f1 = simpson_integrand(t, p, k + 1, tau),
+                   f2 = simpson_integrand(t, p, k + 2, tau);
+      acc.add(hs / 6.0 * (f0 * (2.0 - 1.0 / r) + f1 * (hs * hs / hp) + f2 * (2.0 - r)));
+    }
+  }
+  ss[threadIdx.x] = acc.s;
+  cs[threadIdx.x] = acc.c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    Kahan tot{0.0, 0.0};
+    for (int k = 0; k < (int)blockDim.x; ++k) {
+      tot.add(ss[k]);
+      tot.add(cs[k]);
+    }
+    if (n == 2) {
+      tot.add(0.5 * (t[1] - t[0]) * (simpson_integrand(t, p, 0, tau) + simpson_integrand(t, p, 1, tau)));
+    } else if (n % 2 == 0 && n >= 4) {
+      const double a = t[n - 2] - t[n - 3], b = t[n - 1] - t[n - 2];
+      const double al = (2 * b * b + 3 * a * b) / (6 * (a + b));
+      const double be = (b * b + 3 * a * b) / (6 * a);
+      const double et = b * b * b / (6 * a * (a + b));
+      tot.add(al * simpson_integrand(t, p, n - 1, tau));
+      tot.add(be * simpson_integrand(t, p, n - 2, tau));
+      tot.add(-et * simpson_integrand(t, p, n - 3, tau));
+    }
+    out[blockIdx.x] = tot.s + tot.c;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+static LanczosScalars* scalars(rpm_system* sys) {
+  return static_cast<LanczosScalars*>(system_scratch(sys, SLOT_SMALL, sizeof(LanczosScalars)));
+}
+
+static double2* reduce_partials(rpm_system* sys, size_t count) {
+  return static_cast<double2*>(system_scratch(sys, SLOT_REDUCE, count * sizeof(double2)));
+}
+
+static int row_blocks(long long n) { return (int)((n + kRowsPerBlock - 1) / kRowsPerBlock); }
+
+void lanczos_basis(rpm_system* sys, const double2* state, int max_dim, double tol, double2* basis, double* alpha,
+                   double* beta, int* actual, double* norm, cudaStream_t st) {
+  const long long n = sys->n;
+  const int m = (int)std::min<long long>(max_dim, n);
+  if (m < 1 || m > RPM_MAX_KRYLOV) fail(RPM_E_UNSUPPORTED, "Krylov dimension must be in [1, 128]");
+  LanczosScalars* sc = scalars(sys);
+  const int nb = row_blocks(n);
+  double2* partials = reduce_partials(sys, (size_t)nb * (RPM_MAX_KRYLOV + 1));
+  double2* w = static_cast<double2*>(system_scratch(sys, SLOT_WORK, (size_t)n * sizeof(double2)));
+  const int ew_blocks = (int)std::min<long long>((n + 255) / 256, 4096);
+
+  k_norm_partial<<<nb, kThreads, 0, st>>>(state, n, partials, sc, 1);
+  k_scale_to<<<ew_blocks, 256, 0, st>>>(state, basis, n, sc);
+  check_launch("lanczos init");
+  for (int j = 0; j < m; ++j) {
+    double2* vj = basis + (size_t)j * n;
+    launch_hpsi<double2>(sys, vj, w, 1, n, st);
+    k_alpha<<<nb, kThreads, 0, st>>>(vj, w, n, partials, sc, alpha, j);
+    k_update_dots<<<nb, kThreads, 0, st>>>(basis, w, n, j, alpha, beta, partials, sc);
+    k_axpy_then<<<nb, kThreads, 0, st>>>(basis, w, n, j, 1, 0, tol, beta, partials, sc);
+    k_axpy_then<<<nb, kThreads, 0, st>>>(basis, w, n, j, 0, j == m - 1, tol, beta, partials, sc);
+    if (j + 1 < m) k_next_vector<<<ew_blocks, 256, 0, st>>>(w, basis + (size_t)(j + 1) * n, n, beta, j, sc);
+    check_launch("lanczos step");
+  }
+  struct {
+    int stop;
+    int pad;
+    double norm;
+  } info;
+  check_cuda(cudaMemcpyAsync(&info, &sc->stop, sizeof(info), cudaMemcpyDeviceToHost, st), "copy lanczos info");
+  check_cuda(cudaStreamSynchronize(st), "lanczos sync");
+  *norm = info.norm;
+  if (info.stop < 0) fail(RPM_E_INVALID, "Cannot propagate the zero vector.");
+  *actual = info.stop > 0 ? info.stop : m;
+}
+
+}  // namespace rpm
+
+using namespace rpm;
+
+extern "C" {
+
+int rpm_lanczos_basis(rpm_system* sys, const void* state_dev, int max_dim, double breakdown_tol, void* basis_dev,
+                      double* alpha_dev, double* beta_dev, int* actual_host, double* norm_host, void* stream) {
+  return guarded([&] {
+    if (!sys || !state_dev || !basis_dev || !alpha_dev || !beta_dev || !actual_host || !norm_host)
+      fail(RPM_E_INVALID, "NULL argument");
+    if (!sys->on_device) fail(RPM_E_INVALID, "system was created host-only");
+    lanczos_basis(sys, static_cast<const double2*>(state_dev), max_dim, breakdown_tol, static_cast<double2*>(basis_dev),
+                  alpha_dev, beta_dev, actual_host, norm_host, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int rpm_tridiag_spectra(const double* alpha_dev, const double* beta_dev, int ndims, const int* dims_host,
+                        double* spectra_dev, void* stream) {
+  return guarded([&] {
+    if (!alpha_dev || !beta_dev || !dims_host || !spectra_dev || ndims < 1) fail(RPM_E_INVALID, "bad arguments");
+    for (int k = 0; k < ndims; ++k)
+      if (dims_host[k] < 1 || dims_host[k] > RPM_MAX_KRYLOV) fail(RPM_E_UNSUPPORTED, "Krylov dimension must be in [1, 128]");
+    auto st = static_cast<cudaStream_t>(stream);
+    int* d_dims = nullptr;
+    check_cuda(cudaMallocAsync(&d_dims, sizeof(int) * ndims, st), "cudaMallocAsync(dims)");
+    check_cuda(cudaMemcpyAsync(d_dims, dims_host, sizeof(int) * ndims, cudaMemcpyHostToDevice, st), "copy dims");
+    const size_t smem = sizeof(double) * (RPM_MAX_KRYLOV * RPM_MAX_KRYLOV + 2 * RPM_MAX_KRYLOV) +
+                        sizeof(double2) * RPM_MAX_KRYLOV;
+    check_cuda(cudaFuncSetAttribute(k_tridiag_spectra, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+               "cudaFuncSetAttribute(spectra)");
+    k_tridiag_spectra<<<ndims, 128, smem, st>>>(alpha_dev, beta_dev, d_dims, spectra_dev);
+    check_launch("k_tridiag_spectra");
+    check_cuda(cudaFreeAsync(d_dims, st), "cudaFreeAsync(dims)");
+  });
+}
+
+int rpm_krylov_eval(const double* spectra_dev, int nreq, const rpm_krylov_req* reqs_host, double safety,
+                    double state_norm, const void* gram_dev, int gram_ld, void* coef_dev, int coef_ld,
+                    double* err_host, double* value_host, void* stream) {
+  return guarded([&] {
+    if (!spectra_dev || nreq < 1 || !reqs_host || !coef_dev || !err_host) fail(RPM_E_INVALID, "bad arguments");
+    if (gram_dev && !value_host) fail(RPM_E_INVALID, "value_host required with a Gram matrix");
+    auto st = static_cast<cudaStream_t>(stream);
+    const size_t req_bytes = sizeof(rpm_krylov_req) * nreq;
+    void* dbuf = nullptr;
+    check_cuda(cudaMallocAsync(&dbuf, req_bytes + sizeof(double) * 2 * nreq, st), "cudaMallocAsync(eval)");
+    auto* d_req = static_cast<rpm_krylov_req*>(dbuf);
+    auto* d_err = reinterpret_cast<double*>(static_cast<char*>(dbuf) + req_bytes);
+    double* d_val = d_err + nreq;
+    check_cuda(cudaMemcpyAsync(d_req, reqs_host, req_bytes, cudaMemcpyHostToDevice, st), "copy reqs");
+    k_krylov_eval<<<nreq, kThreads, 0, st>>>(spectra_dev, d_req, safety, state_norm,
+                                              static_cast<const double2*>(gram_dev), gram_ld,
+                                              static_cast<double2*>(coef_dev), coef_ld, d_err, d_val);
+    check_launch("k_krylov_eval");
+    check_cuda(cudaMemcpyAsync(err_host, d_err, sizeof(double) * nreq, cudaMemcpyDeviceToHost, st), "copy err");
+    if (gram_dev)
+      check_cuda(cudaMemcpyAsync(value_host, d_val, sizeof(double) * nreq, cudaMemcpyDeviceToHost, st), "copy values");
+    check_cuda(cudaFreeAsync(dbuf, st), "cudaFreeAsync(eval)");
+    check_cuda(cudaStreamSynchronize(st), "eval sync");
+  });
+}
+
+int rpm_singlet_gram(rpm_system* sys, const void* basis_dev, int m, void* gram_dev, void* stream) {
+  return guarded([&] {
+    if (!sys || !basis_dev || !gram_dev) fail(RPM_E_INVALID, "NULL argument");
+    if (m < 1 || m > 64) fail(RPM_E_UNSUPPORTED, "Gram size must be in [1, 64]");
+    if (sys->ndims < 2 || sys->dims[0] != 2 || sys->dims[1] != 2)
+      fail(RPM_E_INVALID, "The first two axes must be the two electron spins.");
+    auto st = static_cast<cudaStream_t>(stream);
+    const long long quarter = sys->n / 4;
+    int blocks = (int)std::min<long long>((quarter + kGramRows - 1) / kGramRows, 2 * 148);
+    blocks = std::max(blocks, 1);
+    auto* partials = static_cast<double2*>(system_scratch(sys, SLOT_GRAM, (size_t)blocks * m * m * sizeof(double2)));
+    const size_t smem = (size_t)kGramRows * m * sizeof(double2);
+    k_gram_partial<<<blocks, kThreads, smem, st>>>(static_cast<const double2*>(basis_dev), sys->n, m, partials);
+    k_gram_finish<<<(m * m + 255) / 256, 256, 0, st>>>(partials, blocks, m, static_cast<double2*>(gram_dev));
+    check_launch("singlet gram");
+  });
+}
+
+int rpm_combine(rpm_system* sys, const void* basis_dev, int m, const void* coef_dev, double scale, void* out_dev,
+                double* norm_host, void* stream) {
+  return guarded([&] {
+    if (!sys || !basis_dev || !coef_dev || !out_dev) fail(RPM_E_INVALID, "NULL argument");
+    if (m < 1 || m > RPM_MAX_KRYLOV) fail(RPM_E_UNSUPPORTED, "Krylov dimension must be in [1, 128]");
+    auto st = static_cast<cudaStream_t>(stream);
+    const int nb = row_blocks(sys->n);
+    double2* partials = reduce_partials(sys, (size_t)nb * (RPM_MAX_KRYLOV + 1));
+    LanczosScalars* sc = scalars(sys);
+    k_combine<<<nb, kThreads, 0, st>>>(static_cast<const double2*>(basis_dev), sys->n, m,
+                                       static_cast<const double2*>(coef_dev), scale, static_cast<double2*>(out_dev),
+                                       partials, &sc->counter[5], &sc->norm);
+    check_launch("k_combine");
+    if (norm_host) {
+      check_cuda(cudaMemcpyAsync(norm_host, &sc->norm, sizeof(double), cudaMemcpyDeviceToHost, st), "copy norm");
+      check_cuda(cudaStreamSynchronize(st), "combine sync");
+    }
+  });
+}
+
+static int batch_reduce(long long n, const void* psi, int batch, long long ld, int kind, double* host,
+                        void* stream) {
+  return guarded([&] {
+    if (!psi || !host || batch < 1 || n < 1 || ld < n) fail(RPM_E_INVALID, "bad arguments");
+    if (kind == 1 && n % 4 != 0) fail(RPM_E_INVALID, "The first two axes must be the two electron spins.");
+    auto st = static_cast<cudaStream_t>(stream);
+    double* d_out = nullptr;
+    check_cuda(cudaMallocAsync(&d_out, sizeof(double) * batch, st), "cudaMallocAsync(reduce)");
+    k_batch_reduce<<<batch, kThreads, 0, st>>>(static_cast<const double2*>(psi), n, ld, kind, d_out);
+    check_launch("k_batch_reduce");
+    check_cuda(cudaMemcpyAsync(host, d_out, sizeof(double) * batch, cudaMemcpyDeviceToHost, st), "copy reduce");
+    check_cuda(cudaFreeAsync(d_out, st), "cudaFreeAsync(reduce)");
+    check_cuda(cudaStreamSynchronize(st), "reduce sync");
+  });
+}
+
+int rpm_singlet_population(const void* psi_dev, long long n, int batch, long long ld, double* values_host,
+                           void* stream) {
+  return batch_reduce(n, psi_dev, batch, ld, 1, values_host, stream);
+}
+
+int rpm_norm(rpm_system* sys, const void* psi_dev, double* norm_host, void* stream) {
+  if (!sys) {
+    set_last_error("system is NULL");
+    return RPM_E_INVALID;
+  }
+  const int rc = batch_reduce(sys->n, psi_dev, 1, sys->n, 0, norm_host, stream);
+  if (rc == RPM_OK) *norm_host = std::sqrt(*norm_host);
+  return rc;
+}
+
+int rpm_simpson_yield(const double* times_dev, const double* pops_dev, int n, int batch, long long ld,
+                      double lifetime_us, double* yields_dev, void* stream) {
+  return guarded([&] {
+    if (!times_dev || !pops_dev || !yields_dev || n < 1 || batch < 1 || ld < n || !(lifetime_us > 0.0))
+      fail(RPM_E_INVALID, "bad arguments");
+    auto st = static_cast<cudaStream_t>(stream);
+    k_simpson<<<batch, kThreads, 0, st>>>(times_dev, pops_dev, n, ld, lifetime_us, yields_dev);
+    check_launch("k_simpson");
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,131 @@
+"""Host-side checks that need no GPU: the C ABI library, its host-built
+radical-split tables, and the Python model/assembly code."""
+
+import ctypes
+import math
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import REPO, terms_from
+from rpm_b200 import _lib, model, synthetic
+from rpm_b200.engine import LocalTerm, _auto_split, _DeviceSystem
+
+
+def header_functions():
+    text = (REPO / "include" / "rpm_b200.h").read_text()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(rpm_\w+)\s*\(", text, flags=re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    declared = header_functions()
+    assert len(declared) >= 15
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert set(declared) - {"rpm_last_error"} <= set(_lib.SIGNATURES)
+    assert lib.rpm_version() >= 1
+
+
+def test_device_count_without_gpu_is_a_clean_zero_or_more():
+    assert _lib.device_count() >= 0
+
+
+def _dense_from_csr(ptr, col, val, n):
+    out = np.zeros((n, n), dtype=complex)
+    for r in range(n):
+        for k in range(ptr[r], ptr[r + 1]):
+            out[r, col[k]] += val[k]
+    return out
+
+
+@pytest.mark.parametrize("key", ["small", "prefix6", "prefix10", "full"])
+def test_split_tables_match_oracle_blocks(golden, key):
+    if key == "full":
+        sysm = synthetic.full_system()
+        dims, left, right = sysm.dimensions, sysm.left_axes, sysm.right_axes
+        terms = sysm.terms(math.pi / 4, 0.0)
+    else:
+        dims = tuple(int(v) for v in golden[f"{key}_dims"])
+        left, right = tuple(golden[f"{key}_left"]), tuple(golden[f"{key}_right"])
+        terms = terms_from(golden, key, LocalTerm)
+    ds = _DeviceSystem(dims, terms, left, right, host_only=True)
+    assert ds.split and ds.n == math.prod(dims)
+    t = ds.split_tables()
+    ref = oracle.CompiledFullPairHamiltonian(dims, [oracle.LocalTerm(x.axes, x.operator) for x in terms],
+                                             left_axes=left, right_axes=right)
+    np.testing.assert_allclose(_dense_from_csr(t["lptr"], t["lcol"], t["lval"], ds.nl), ref.left_operator, atol=1e-13)
+    np.testing.assert_allclose(_dense_from_csr(t["rptr"], t["rcol"], t["rval"], ds.nr), ref.right_operator, atol=1e-13)
+    np.testing.assert_allclose(t["pair"].reshape(2, 2, 2, 2), ref.electron_pair_operator, atol=1e-14)
+    # memory offsets reproduce the reference's axis permutation
+    strides = np.array([math.prod(dims[a + 1:]) for a in range(len(dims))])
+    grid_l = np.indices(ref.left_dimensions).reshape(len(left), -1)
+    grid_r = np.indices(ref.right_dimensions).reshape(len(right), -1)
+    np.testing.assert_array_equal(t["offl"], (strides[list(left)][:, None] * grid_l).sum(0))
+    np.testing.assert_array_equal(t["offr"], (strides[list(right)][:, None] * grid_r).sum(0))
+
+
+def test_host_only_system_rejects_bad_terms():
+    sx = model.spin_operators(0.5)[0]
+    with pytest.raises(ValueError, match="unique active axes"):
+        _DeviceSystem((2, 2), [LocalTerm((0, 0), np.kron(sx, sx))], host_only=True)
+    with pytest.raises(ValueError, match="out-of-range"):
+        _DeviceSystem((2, 2), [LocalTerm((2,), sx)], host_only=True)
+    with pytest.raises(ValueError, match="not Hermitian"):
+        _DeviceSystem((2, 2), [LocalTerm((0,), np.array([[0, 1], [0, 0]], dtype=complex))], host_only=True)
+    with pytest.raises(ValueError, match="Cross-radical"):
+        _DeviceSystem((2, 2, 2), [LocalTerm((0, 2), np.kron(sx, sx))], (0,), (1, 2), host_only=True)
+    with pytest.raises(ValueError, match="partition"):
+        _DeviceSystem((2, 2, 2), [], (0,), (1,), host_only=True)
+
+
+def test_auto_split_detection():
+    sm = synthetic.small_system()
+    terms = sm.terms(0.3, 0.2)
+    assert _auto_split(sm.dimensions, terms) == (sm.left_axes, sm.right_axes)
+    sx = model.spin_operators(0.5)[0]
+    # a nuclear-nuclear coupling across radicals forbids a split
+    bad = terms + [LocalTerm((2, 4), np.kron(model.spin_operators(1.0)[0], sx))]
+    assert _auto_split(sm.dimensions, bad) is None
+
+
+def test_model_builders_match_reference_outputs(golden):
+    for s in (0.5, 1.0, 1.5):
+        for name, op in zip("xyz", model.spin_operators(s)):
+            np.testing.assert_allclose(op, golden[f"spin_{s}_{name}"], atol=1e-15)
+    t = golden["coupling_tensor"]
+    np.testing.assert_allclose(model.two_spin_coupling_operator(0.5, 1.0, t), golden["coupling_half_one"], atol=1e-14)
+    np.testing.assert_allclose(model.quadrupole_operator(1.0, golden["quad_tensor"]), golden["quad_one"], atol=1e-14)
+    np.testing.assert_allclose(model.efimova_hore_electron_coupling_operator(1.7, -2.3, golden["eh_axis"]),
+                               golden["eh_op"], atol=1e-14)
+    for key, tensor in model.QUADRUPOLE_TENSORS_MT.items():
+        np.testing.assert_allclose(tensor, golden[f"qtensor_{key}"], atol=1e-15)
+    for k, nuc in enumerate(model.ALL_NUCLEI):
+        np.testing.assert_array_equal(nuc.tensor_mT, golden[f"hf_{k}"])
+
+
+def test_production_seeds_and_states(golden):
+    from rpm_b200 import production
+
+    assert [production._seed(20260731, s) for s in range(4)] == [int(v) for v in golden["seeds"]]
+    init = production.random_phase_initial_state(model.SYSTEM_DIMENSIONS, 20260731, 0)
+    np.testing.assert_allclose(init[golden["init_s0_checks_idx"]], golden["init_s0_checks_val"], atol=1e-15)
+    grid = production.time_grid_us(production.maximum_time_us(5.0, 1e-5))
+    assert grid[-1] == pytest.approx(57.564627324851145, abs=1e-12)
+    idx = production.coarse_grid_indices(grid.size)
+    assert idx[0] == 0 and idx[-1] == grid.size - 1
+
+
+def test_synthetic_systems_have_reference_shapes():
+    full = synthetic.full_system()
+    assert full.dimensions == model.SYSTEM_DIMENSIONS
+    assert synthetic.small_system().dimension == 96
+    assert synthetic.prefix_system(full, 3).dimension == 864
+    assert synthetic.prefix_system(full, 5).dimension == 13824
+    for t in full.terms(0.4, 1.3):
+        np.testing.assert_allclose(t.operator, t.operator.conj().T, atol=1e-12)
+    dirs = synthetic.fibonacci_sphere(12)
+    assert len(dirs) == 12 and all(0 <= th <= math.pi for th, _ in dirs)
