@@ -143,6 +143,57 @@ int rpm_norm(rpm_system* sys, const void* psi_dev, double* norm_host, void* stre
 int rpm_simpson_yield(const double* times_dev, const double* pops_dev, int n, int batch,
                       long long ld, double lifetime_us, double* yields_dev, void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Batched mixed-precision propagation: many trajectories (state vectors of
+ * one or more systems, e.g. field orientations or bath sizes) advanced
+ * together.  complex64 Lanczos basis and H psi; FP64 alpha/beta, state,
+ * tridiagonal exponential, error control and singlet populations.  The
+ * batched counterpart of ENG:717-933 (AdaptiveLanczosPropagator.propagate
+ * with SingletPopulationObservable) with a fixed Krylov dimension and the
+ * largest step meeting the embedded error budget (no rejected steps).
+ * ------------------------------------------------------------------------- */
+typedef struct rpm_batch rpm_batch;
+
+typedef struct rpm_batch_config {
+  int krylov_dim;              /* fixed Krylov dimension, 2..64              */
+  int embedded_offset;         /* error estimate from dims (m, m - offset)   */
+  double safety_factor;        /* multiplies the embedded estimate           */
+  double state_error_budget;   /* total over [0, T], allotted per dt/T       */
+  double initial_step_us;      /* first trial step                           */
+  double maximum_step_us;
+  double minimum_step_us;      /* below this a trajectory fails (status 3)   */
+  double breakdown_relative;   /* beta_j <= rel*(|alpha_j|+beta_{j-1}): stop */
+  int use_graph;               /* replay each Krylov step from a CUDA graph   */
+  long long max_steps;         /* safety limit on Krylov steps (<=0: 1e7)    */
+} rpm_batch_config;
+
+typedef struct rpm_batch_stats {
+  int accepted_steps;
+  int rejected_steps;
+  long long matvecs;
+  int maximum_krylov_dimension;
+  int status;                  /* 0 ok, 1 zero/non-finite input, 2 eigen-solver,
+                                  3 step underflow, 4 non-finite state        */
+  double minimum_step_us;
+  double maximum_step_us;
+  double accumulated_state_error;
+  double maximum_norm_error;
+} rpm_batch_stats;
+
+/* Prepare a batch over `nsys` radical-split systems (each must have the cube
+ * form: terms on {e}, {n_k} or {e, n_k} per radical). */
+int rpm_batch_create(rpm_system* const* systems, int nsys, const rpm_batch_config* cfg, rpm_batch** out);
+/* Per-trajectory stride (elements) of the state buffer passed to propagate. */
+int rpm_batch_leading_dimension(const rpm_batch* batch, long long* ld);
+/* Propagate `ntraj` trajectories; trajectory b uses system sys_of_host[b] and
+ * starts from psi_dev + b*ld (complex128, overwritten with the final state).
+ * values_dev / state_errors_dev (ntraj x ntimes, FP64, device) receive the
+ * singlet population and the accumulated state-error estimate at each time. */
+int rpm_batch_propagate(rpm_batch* batch, int ntraj, const int* sys_of_host, void* psi_dev,
+                        const double* times_host, int ntimes, double* values_dev,
+                        double* state_errors_dev, rpm_batch_stats* stats_host, void* stream);
+int rpm_batch_destroy(rpm_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

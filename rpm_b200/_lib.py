@@ -50,6 +50,21 @@ class rpm_krylov_req(ctypes.Structure):
     _fields_ = [("hi", ctypes.c_int), ("lo", ctypes.c_int), ("time", ctypes.c_double)]
 
 
+class rpm_batch_config(ctypes.Structure):
+    _fields_ = [("krylov_dim", ctypes.c_int), ("embedded_offset", ctypes.c_int), ("safety_factor", ctypes.c_double),
+                ("state_error_budget", ctypes.c_double), ("initial_step_us", ctypes.c_double),
+                ("maximum_step_us", ctypes.c_double), ("minimum_step_us", ctypes.c_double),
+                ("breakdown_relative", ctypes.c_double), ("use_graph", ctypes.c_int),
+                ("max_steps", ctypes.c_longlong)]
+
+
+class rpm_batch_stats(ctypes.Structure):
+    _fields_ = [("accepted_steps", ctypes.c_int), ("rejected_steps", ctypes.c_int), ("matvecs", ctypes.c_longlong),
+                ("maximum_krylov_dimension", ctypes.c_int), ("status", ctypes.c_int),
+                ("minimum_step_us", ctypes.c_double), ("maximum_step_us", ctypes.c_double),
+                ("accumulated_state_error", ctypes.c_double), ("maximum_norm_error", ctypes.c_double)]
+
+
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _LL = ctypes.c_longlong
@@ -75,6 +90,10 @@ SIGNATURES: dict[str, list] = {
     "rpm_singlet_population": [_P, _LL, _I, _LL, _PD, _P],
     "rpm_norm": [_P, _P, _PD, _P],
     "rpm_simpson_yield": [_P, _P, _I, _I, _LL, _D, _P, _P],
+    "rpm_batch_create": [ctypes.POINTER(_P), _I, ctypes.POINTER(rpm_batch_config), ctypes.POINTER(_P)],
+    "rpm_batch_leading_dimension": [_P, _PLL],
+    "rpm_batch_propagate": [_P, _I, _PI, _P, _PD, _I, _P, _P, ctypes.POINTER(rpm_batch_stats), _P],
+    "rpm_batch_destroy": [_P],
 }
 
 _lib = None

@@ -1,0 +1,799 @@
+// Batched mixed-precision Krylov propagation (many trajectories per launch).
+//
+// One "trajectory" is one state vector of one system (field orientation /
+// system size) propagated over the observation grid.  Precision follows the
+// split the hot path needs:
+//   * the Lanczos basis and every H psi are complex64 with FP32 accumulation;
+//   * alpha/beta reductions, the state between Krylov steps (complex128),
+//     its recombination psi = ||psi|| V c, the tridiagonal eigen-solve,
+//     exp(-i T t) e1, the error control and the singlet Gram/populations are
+//     FP64.
+// Each Krylov step is a fixed kernel sequence over all trajectories:
+//   start -> m x [H psi (pass L, pass R + alpha), update + beta]
+//         -> control -> rebuild -> gram -> observe
+// captured once as a CUDA graph and replayed until every trajectory reached
+// the last observation time.  Per-trajectory controller state lives on the
+// device; the host only polls a done-counter.
+//
+// Step control (per trajectory): with the Krylov basis of dimension m fixed,
+// the embedded error err(dt) = safety * ||psi|| * ||c_m(dt) - [c_{m-off}(dt); 0]||
+// (the reference's estimate, rpm_statevector_engine.py:690-715) is evaluated
+// for trial steps, and the largest dt <= min(max_step, T - t) with
+// err(dt) <= budget * dt / T is taken.  Because the basis does not depend on
+// dt, no step is ever rejected.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <memory>
+
+#include "common.cuh"
+#include "hpsi.cuh"
+#include "krylov.cuh"
+
+namespace rpm {
+
+constexpr int kBMaxK = 64;    // Krylov dimension cap of the batched path
+constexpr int kMaxPts = 256;  // observation points per Krylov step
+constexpr int kEwThreads = 256;
+constexpr int kEwPer = 8;                         // elements per thread
+constexpr int kEwChunk = kEwThreads * kEwPer;     // elements per block
+constexpr int kRecDoubles = 2 + kBMaxK + kBMaxK * kBMaxK;  // one spectra record (LD = kBMaxK)
+
+struct TrajState {
+  double t_now, dt, norm, new_norm2, acc_err, step_err, max_norm_err;
+  double min_step, max_step, hint, scale;
+  double alpha[kBMaxK];
+  double beta[kBMaxK];
+  long long n, matvecs;
+  int cursor, npts, done, stop, skip, msize, steps, sys;
+  int status, pad_;
+};
+static_assert(sizeof(TrajState) % 8 == 0, "TrajState must be a whole number of doubles");
+static_assert(sizeof(TrajState) % 4 == 0, "TrajState must be a whole number of ints");
+constexpr int kStateDoubles = sizeof(TrajState) / 8;
+constexpr int kStateInts = sizeof(TrajState) / 4;
+
+struct BatchDev {
+  TrajState* st;
+  int ntraj, m, offset;
+  double safety, budget, max_step, min_step, t_end, breakdown_rel;
+  const double* times;
+  int ntimes;
+  long long ld;
+  float2* V;        // [traj][m + 1][ld]
+  double2* psi;     // [traj][ld]
+  double2* coef;    // [traj][kMaxPts + 1][kBMaxK]; row kMaxPts = endpoint
+  double* perr;     // [traj][kMaxPts]
+  double* part;     // [traj][nblk][2]
+  unsigned* count;  // [traj] completion counters (elementwise reductions)
+  double2* gpart;   // [traj][gblk][kBMaxK * kBMaxK]
+  double* values;   // [traj][ntimes]
+  double* errs;     // [traj][ntimes]
+  int nblk, gblk;
+  int* active;      // trajectories not yet done
+};
+
+__device__ __forceinline__ bool traj_last_block(unsigned* counter) {
+  __shared__ bool is_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) is_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (is_last) __threadfence();
+  return is_last;
+}
+
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  v = warp_sum(v);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+  return s;
+}
+
+// Sum two partial slots over the blocks of trajectory b, in block order.
+__device__ __forceinline__ double2 sum_parts(const BatchDev& B, int b) {
+  double2 s = make_double2(0.0, 0.0);
+  const double* p = B.part + (size_t)b * B.nblk * 2;
+  for (int k = 0; k < (int)gridDim.x; ++k) {
+    s.x += __ldcg(p + 2 * k);
+    s.y += __ldcg(p + 2 * k + 1);
+  }
+  return s;
+}
+
+// ---------------------------------------------------------------------------
+// Set-up: state fields, ||psi0|| and P_S(psi0)
+// ---------------------------------------------------------------------------
+__global__ void k_b_setup(BatchDev B, const int* sys_of, const long long* n_of, double initial_step) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B.ntraj) return;
+  TrajState& s = B.st[b];
+  int* raw = reinterpret_cast<int*>(&s);
+  for (int k = 0; k < kStateInts; ++k) raw[k] = 0;
+  s.sys = sys_of[b];
+  s.n = n_of[b];
+  s.hint = initial_step;
+  s.min_step = DBL_MAX;
+  s.msize = B.m;
+  s.scale = 1.0;
+  B.count[b] = 0;
+}
+
+__global__ void __launch_bounds__(kEwThreads) k_b_init(BatchDev B) {
+  __shared__ double red[32];
+  const int b = blockIdx.y;
+  TrajState& s = B.st[b];
+  const long long n = s.n, q = n / 4;
+  const double2* x = B.psi + (size_t)b * B.ld;
+  double nn = 0.0, ps = 0.0;
+  for (long long i = (long long)blockIdx.x * kEwChunk + threadIdx.x; i < n && i < (long long)(blockIdx.x + 1) * kEwChunk;
+       i += kEwThreads) {
+    const double2 v = x[i];
+    nn = fma(v.x, v.x, fma(v.y, v.y, nn));
+    if (i >= q && i < 2 * q) {
+      const double2 w = x[i + q];
+      const double re = v.x - w.x, im = v.y - w.y;
+      ps = fma(re, re, fma(im, im, ps));
+    }
+  }
+  nn = block_sum(nn, red);
+  ps = block_sum(ps, red);
+  if (threadIdx.x == 0) {
+    B.part[((size_t)b * B.nblk + blockIdx.x) * 2] = nn;
+    B.part[((size_t)b * B.nblk + blockIdx.x) * 2 + 1] = 0.5 * ps;
+  }
+  if (traj_last_block(B.count + b) && threadIdx.x == 0) {
+    const double2 tot = sum_parts(B, b);
+    s.norm = sqrt(tot.x);
+    s.max_norm_err = fabs(s.norm - 1.0);
+    if (B.times[0] == 0.0) {
+      B.values[(size_t)b * B.ntimes] = tot.y;
+      B.errs[(size_t)b * B.ntimes] = 0.0;
+      s.cursor = 1;
+    }
+    if (!(s.norm > 0.0) || !isfinite(s.norm)) {
+      s.status = 1;
+      s.done = 1;
+    }
+    if (s.cursor >= B.ntimes) s.done = 1;
+    s.skip = s.done;
+    if (s.done) atomicSub(B.active, 1);
+    B.count[b] = 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Krylov step kernels
+// ---------------------------------------------------------------------------
+// v0 = psi / ||psi|| (complex64)
+__global__ void __launch_bounds__(kEwThreads) k_b_start(BatchDev B) {
+  const int b = blockIdx.y;
+  TrajState& s = B.st[b];
+  if (s.done) return;
+  const double inv = 1.0 / s.norm;
+  const double2* x = B.psi + (size_t)b * B.ld;
+  float2* v0 = B.V + (size_t)b * (B.m + 1) * B.ld;
+  const long long end = min(s.n, (long long)(blockIdx.x + 1) * kEwChunk);
+  for (long long i = (long long)blockIdx.x * kEwChunk + threadIdx.x; i < end; i += kEwThreads) {
+    const double2 v = x[i];
+    v0[i] = make_float2((float)(v.x * inv), (float)(v.y * inv));
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    s.stop = 0;
+    s.skip = 0;
+    s.msize = B.m;
+    s.scale = 1.0;
+  }
+}
+
+// v_j <- scale * V_j (in place);  w = V_{j+1} - alpha_j v_j - beta_{j-1} v_{j-1};
+// beta_j = ||w||, scale = 1 / beta_j; breakdown when beta_j is at round-off level.
+__global__ void __launch_bounds__(kEwThreads) k_b_update(BatchDev B, int j) {
+  __shared__ double red[32];
+  const int b = blockIdx.y;
+  TrajState& s = B.st[b];
+  if (s.skip) return;
+  const float sc = (float)s.scale;
+  const float a = (float)s.alpha[j];
+  const float bp = j > 0 ? (float)s.beta[j - 1] : 0.0f;
+  float2* base = B.V + (size_t)b * (B.m + 1) * B.ld;
+  float2* vj = base + (size_t)j * B.ld;
+  float2* wn = base + (size_t)(j + 1) * B.ld;
+  const float2* vp = base + (size_t)(j > 0 ? j - 1 : 0) * B.ld;
+  const bool last = (j == B.m - 1);
+  double nn = 0.0;
+  const long long end = min(s.n, (long long)(blockIdx.x + 1) * kEwChunk);
+  for (long long i = (long long)blockIdx.x * kEwChunk + threadIdx.x; i < end; i += kEwThreads) {
+    float2 v = vj[i];
+    v.x *= sc;
+    v.y *= sc;
+    vj[i] = v;
+    if (!last) {
+      float2 w = wn[i];
+      w.x = fmaf(-a, v.x, w.x);
+      w.y = fmaf(-a, v.y, w.y);
+      if (j > 0) {
+        const float2 u = vp[i];
+        w.x = fmaf(-bp, u.x, w.x);
+        w.y = fmaf(-bp, u.y, w.y);
+      }
+      wn[i] = w;
+      nn = fma((double)w.x, (double)w.x, fma((double)w.y, (double)w.y, nn));
+    }
+  }
+  if (last) return;
+  nn = block_sum(nn, red);
+  if (threadIdx.x == 0) B.part[((size_t)b * B.nblk + blockIdx.x) * 2] = nn;
+  if (traj_last_block(B.count + b) && threadIdx.x == 0) {
+    double tot = 0.0;
+    const double* p = B.part + (size_t)b * B.nblk * 2;
+    for (int k = 0; k < (int)gridDim.x; ++k) tot += __ldcg(p + 2 * k);
+    const double bj = sqrt(tot);
+    s.beta[j] = bj;
+    s.scale = bj > 0.0 ? 1.0 / bj : 0.0;
+    const double ref = fabs(s.alpha[j]) + (j > 0 ? s.beta[j - 1] : 0.0);
+    if (!(bj > B.breakdown_rel * ref)) {
+      s.stop = 1;
+      s.skip = 1;
+      s.msize = j + 1;
+    }
+    B.count[b] = 0;
+  }
+}
+
+// Embedded error of the step dt; `c` receives c_hi(dt) (m entries).
+__device__ double step_error(const double* rec_hi, const double* rec_lo, bool exact, double dt, double safety,
+                             double norm, double2* ph, double2* c, double2* clo, double* red) {
+  spectral_coefficients<kBMaxK>(rec_hi, dt, ph, c);
+  if (exact) return 0.0;
+  spectral_coefficients<kBMaxK>(rec_lo, dt, ph, clo);
+  const int mh = (int)rec_hi[0], ml = (int)rec_lo[0];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < mh; i += blockDim.x) {
+    double2 d = c[i];
+    if (i < ml) {
+      d.x -= clo[i].x;
+      d.y -= clo[i].y;
+    }
+    acc = fma(d.x, d.x, fma(d.y, d.y, acc));
+  }
+  acc = block_sum(acc, red);
+  return safety * norm * sqrt(acc);
+}
+
+// Per-trajectory controller: eigen-solves, step search, coefficient rows.
+// Dynamic shared memory: two spectra records (hi, lo) of the krylov.cuh layout.
+__global__ void __launch_bounds__(128) k_b_control(BatchDev B) {
+  extern __shared__ double sm[];
+  __shared__ double2 ph[kBMaxK], c[kBMaxK], clo[kBMaxK], rot[kBMaxK];
+  __shared__ double d[kBMaxK], e[kBMaxK], red[32];
+  __shared__ double s_dt;
+  __shared__ int s_ok;
+  const int b = blockIdx.x;
+  TrajState& s = B.st[b];
+  if (s.done) return;
+  double* rec_hi = sm;
+  double* rec_lo = sm + kRecDoubles;
+  const int M = s.msize;
+  const bool exact = s.stop != 0;
+  const int ML = max(1, M - B.offset);
+  // spectra of T_M and T_ML, written in the krylov.cuh record layout
+  for (int pass = 0; pass < (exact ? 1 : 2); ++pass) {
+    const int dim = pass == 0 ? M : ML;
+    double* rec = pass == 0 ? rec_hi : rec_lo;
+    for (int i = threadIdx.x; i < dim; i += blockDim.x) {
+      d[i] = s.alpha[i];
+      e[i] = (i + 1 < dim) ? s.beta[i] : 0.0;
+    }
+    __syncthreads();
+    double* z = rec + 2 + kBMaxK;
+    const int bad = tridiag_qr(dim, d, e, z, kBMaxK, rot);
+    for (int i = threadIdx.x; i < dim; i += blockDim.x) rec[2 + i] = d[i];
+    if (threadIdx.x == 0) {
+      rec[0] = dim;
+      rec[1] = bad;
+      if (bad) s.status = 2;
+    }
+    __syncthreads();
+  }
+  const double t_now = s.t_now;
+  const double remaining = B.t_end - t_now;
+  double dt_max = fmin(B.max_step, remaining);
+  // keep the observation points of one step within the coefficient buffer
+  if (s.cursor + kMaxPts - 1 < B.ntimes) dt_max = fmin(dt_max, B.times[s.cursor + kMaxPts - 1] - t_now);
+  const double norm = s.norm;
+  auto ok = [&](double dt) {
+    const double err = step_error(rec_hi, rec_lo, exact, dt, B.safety, norm, ph, c, clo, red);
+    return err <= B.budget * dt / B.t_end;
+  };
+  if (ok(dt_max)) {
+    if (threadIdx.x == 0) s_dt = dt_max;
+  } else {
+    // bracket [lo, hi] with ok(lo) and !ok(hi), then bisect in log scale
+    double hi = dt_max;
+    double lo = fmin(s.hint, 0.5 * dt_max);
+    int guard = 0;
+    while (!ok(lo) && guard < 60) {
+      hi = lo;
+      lo *= 0.25;
+      ++guard;
+    }
+    if (guard >= 60 || lo < B.min_step) {
+      if (threadIdx.x == 0) {
+        s.status = 3;  // step underflow
+        s.done = 1;
+        s.skip = 1;
+        atomicSub(B.active, 1);
+      }
+      return;
+    }
+    for (int it = 0; it < 24 && hi > lo * 1.0005; ++it) {
+      const double mid = sqrt(lo * hi);
+      if (ok(mid)) lo = mid;
+      else hi = mid;
+    }
+    if (threadIdx.x == 0) s_dt = lo;
+  }
+  __syncthreads();
+  double dt = s_dt;
+  if (remaining - dt < 1e-12) dt = remaining;
+  // endpoint coefficients and error
+  const double err_end = step_error(rec_hi, rec_lo, exact, dt, B.safety, norm, ph, c, clo, red);
+  double2* rows = B.coef + (size_t)b * (kMaxPts + 1) * kBMaxK;
+  for (int i = threadIdx.x; i < kBMaxK; i += blockDim.x) rows[(size_t)kMaxPts * kBMaxK + i] = i < M ? c[i] : make_double2(0, 0);
+  // observation points inside (t_now, t_now + dt]
+  int np = 0;
+  const double t_end_step = t_now + dt;
+  while (s.cursor + np < B.ntimes && np < kMaxPts && B.times[s.cursor + np] <= t_end_step + 1e-13) {
+    const double tau = B.times[s.cursor + np] - t_now;
+    const double perr = step_error(rec_hi, rec_lo, exact, tau, B.safety, norm, ph, c, clo, red);
+    for (int i = threadIdx.x; i < kBMaxK; i += blockDim.x) rows[(size_t)np * kBMaxK + i] = i < M ? c[i] : make_double2(0, 0);
+    if (threadIdx.x == 0) B.perr[(size_t)b * kMaxPts + np] = perr;
+    ++np;
+  }
+  if (threadIdx.x == 0) {
+    s.dt = dt;
+    s.step_err = err_end;
+    s.npts = np;
+  }
+}
+
+// psi = ||psi|| V c_end (FP64 accumulation); ||psi||^2 into new_norm2.
+__global__ void __launch_bounds__(kEwThreads) k_b_rebuild(BatchDev B) {
+  __shared__ double2 cc[kBMaxK];
+  __shared__ double red[32];
+  const int b = blockIdx.y;
+  TrajState& s = B.st[b];
+  if (s.done) return;
+  const int M = s.msize;
+  const double2* row = B.coef + ((size_t)b * (kMaxPts + 1) + kMaxPts) * kBMaxK;
+  for (int k = threadIdx.x; k < M; k += blockDim.x) cc[k] = make_double2(row[k].x * s.norm, row[k].y * s.norm);
+  __syncthreads();
+  const float2* V = B.V + (size_t)b * (B.m + 1) * B.ld;
+  double2* x = B.psi + (size_t)b * B.ld;
+  double nn = 0.0;
+  const long long end = min(s.n, (long long)(blockIdx.x + 1) * kEwChunk);
+  for (long long i = (long long)blockIdx.x * kEwChunk + threadIdx.x; i < end; i += kEwThreads) {
+    double2 acc = make_double2(0.0, 0.0);
+    for (int k = 0; k < M; ++k) {
+      const float2 v = V[(size_t)k * B.ld + i];
+      acc = cfma(cc[k], make_double2(v.x, v.y), acc);
+    }
+    x[i] = acc;
+    nn = fma(acc.x, acc.x, fma(acc.y, acc.y, nn));
+  }
+  nn = block_sum(nn, red);
+  if (threadIdx.x == 0) B.part[((size_t)b * B.nblk + blockIdx.x) * 2] = nn;
+  if (traj_last_block(B.count + b) && threadIdx.x == 0) {
+    double tot = 0.0;
+    const double* p = B.part + (size_t)b * B.nblk * 2;
+    for (int k = 0; k < (int)gridDim.x; ++k) tot += __ldcg(p + 2 * k);
+    s.new_norm2 = tot;
+    B.count[b] = 0;
+  }
+}
+
+// Singlet Gram partials  G_kl = sum_q conj(a_k(q)) a_l(q),
+// a_k(q) = (V_k[n/4 + q] - V_k[n/2 + q]) / sqrt 2, FP32 within a row chunk and
+// FP64 across chunks.
+constexpr int kGramChunk = 32;
+__global__ void __launch_bounds__(256) k_b_gram(BatchDev B) {
+  __shared__ float2 a[kGramChunk * kBMaxK];
+  const int b = blockIdx.y;
+  TrajState& s = B.st[b];
+  if (s.done) return;
+  const int M = s.msize;
+  const long long q4 = s.n / 4;
+  const float2* V = B.V + (size_t)b * (B.m + 1) * B.ld;
+  const int pairs = M * M;
+  double2 acc[16];
+#pragma unroll
+  for (int p = 0; p < 16; ++p) acc[p] = make_double2(0.0, 0.0);
+  const float rs2 = 0.70710678118654752440f;
+  for (long long r0 = (long long)blockIdx.x * kGramChunk; r0 < q4; r0 += (long long)gridDim.x * kGramChunk) {
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kGramChunk * M; idx += blockDim.x) {
+      const int k = idx / kGramChunk, rr = idx % kGramChunk;
+      const long long qq = r0 + rr;
+      float2 v = make_float2(0.f, 0.f);
+      if (qq < q4) {
+        const float2 p1 = V[(size_t)k * B.ld + q4 + qq];
+        const float2 p2 = V[(size_t)k * B.ld + 2 * q4 + qq];
+        v = make_float2((p1.x - p2.x) * rs2, (p1.y - p2.y) * rs2);
+      }
+      a[rr * kBMaxK + k] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < 16; ++p) {
+      const int pr = threadIdx.x + p * blockDim.x;
+      if (pr < pairs) {
+        const int k = pr / M, l = pr % M;
+        float sx = 0.f, sy = 0.f;
+        for (int rr = 0; rr < kGramChunk; ++rr) {
+          const float2 u = a[rr * kBMaxK + k], v = a[rr * kBMaxK + l];
+          sx = fmaf(u.x, v.x, fmaf(u.y, v.y, sx));
+          sy = fmaf(u.x, v.y, fmaf(-u.y, v.x, sy));
+        }
+        acc[p].x += sx;
+        acc[p].y += sy;
+      }
+    }
+  }
+  double2* out = B.gpart + ((size_t)b * B.gblk + blockIdx.x) * kBMaxK * kBMaxK;
+#pragma unroll
+  for (int p = 0; p < 16; ++p) {
+    const int pr = threadIdx.x + p * blockDim.x;
+    if (pr < pairs) out[pr] = acc[p];
+  }
+}
+
+// Populations at the step's observation points and the controller update.
+__global__ void __launch_bounds__(256) k_b_observe(BatchDev B) {
+  extern __shared__ double2 G[];  // M x M
+  const int b = blockIdx.x;
+  TrajState& s = B.st[b];
+  if (s.done) return;
+  const int M = s.msize;
+  const int pairs = M * M;
+  for (int pr = threadIdx.x; pr < pairs; pr += blockDim.x) {
+    double2 t = make_double2(0.0, 0.0);
+    const double2* p = B.gpart + (size_t)b * B.gblk * kBMaxK * kBMaxK + pr;
+    for (int k = 0; k < B.gblk; ++k) t = cadd(t, p[(size_t)k * kBMaxK * kBMaxK]);
+    G[pr] = t;
+  }
+  __syncthreads();
+  const double n2 = s.norm * s.norm;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const double2* rows = B.coef + (size_t)b * (kMaxPts + 1) * kBMaxK;
+  for (int p = warp; p < s.npts; p += nw) {
+    const double2* cv = rows + (size_t)p * kBMaxK;
+    double v = 0.0;
+    for (int i = lane; i < M; i += 32) {
+      // (G c)_i with G Hermitian-symmetrised on the fly
+      double2 gc = make_double2(0.0, 0.0);
+      for (int k = 0; k < M; ++k) {
+        const double2 g1 = G[i * M + k], g2 = G[k * M + i];
+        const double2 g = make_double2(0.5 * (g1.x + g2.x), 0.5 * (g1.y - g2.y));
+        gc = cfma(g, cv[k], gc);
+      }
+      v += cv[i].x * gc.x + cv[i].y * gc.y;
+    }
+    v = warp_sum(v);
+    if (lane == 0) {
+      const int at = s.cursor + p;
+      B.values[(size_t)b * B.ntimes + at] = n2 * v;
+      B.errs[(size_t)b * B.ntimes + at] = s.acc_err + B.perr[(size_t)b * kMaxPts + p];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s.t_now += s.dt;
+    s.cursor += s.npts;
+    s.acc_err += s.step_err;
+    s.steps += 1;
+    s.matvecs += s.msize;
+    s.min_step = fmin(s.min_step, s.dt);
+    s.max_step = fmax(s.max_step, s.dt);
+    s.hint = s.dt;
+    s.norm = sqrt(s.new_norm2);
+    s.max_norm_err = fmax(s.max_norm_err, fabs(s.norm - 1.0));
+    if (!isfinite(s.norm)) s.status = 4;
+    if (s.cursor >= B.ntimes || s.status != 0) {
+      s.done = 1;
+      s.skip = 1;
+      atomicSub(B.active, 1);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+}  // namespace rpm
+
+struct rpm_batch {
+  std::vector<rpm_system*> systems;
+  rpm_batch_config cfg{};
+  rpm::CubePlan plan{};
+  rpm::CubeView<float2>* views_dev = nullptr;
+  long long ld = 0;
+  // buffers (grown on demand)
+  int cap_traj = 0, cap_times = 0;
+  void* buf = nullptr;
+  size_t buf_bytes = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int graph_traj = -1, graph_times = -1;
+  // Work is issued on a private non-blocking stream (graph capture is not
+  // allowed on the legacy default stream), ordered after the caller's stream
+  // on entry and before it on exit through events.
+  cudaStream_t work = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+};
+
+namespace rpm {
+
+static void free_graph(rpm_batch* B) {
+  if (B->exec) cudaGraphExecDestroy(B->exec);
+  if (B->graph) cudaGraphDestroy(B->graph);
+  B->exec = nullptr;
+  B->graph = nullptr;
+  B->graph_traj = B->graph_times = -1;
+}
+
+struct Layout {
+  size_t st, V, coef, perr, part, count, gpart, ya, dotpart, dotcount, times, sysof, nof, active, total;
+};
+
+static Layout layout(const rpm_batch* B, int ntraj, int ntimes, int nblk, int gblk, int dot_blocks) {
+  Layout L{};
+  size_t pos = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = pos;
+    pos += (bytes + 255) & ~(size_t)255;
+    return at;
+  };
+  const int m = B->cfg.krylov_dim;
+  L.st = take(sizeof(TrajState) * ntraj);
+  L.V = take(sizeof(float2) * (size_t)ntraj * (m + 1) * B->ld);
+  L.coef = take(sizeof(double2) * (size_t)ntraj * (kMaxPts + 1) * kBMaxK);
+  L.perr = take(sizeof(double) * (size_t)ntraj * kMaxPts);
+  L.part = take(sizeof(double) * (size_t)ntraj * nblk * 2);
+  L.count = take(sizeof(unsigned) * ntraj);
+  L.gpart = take(sizeof(double2) * (size_t)ntraj * gblk * kBMaxK * kBMaxK);
+  L.ya = take(sizeof(float2) * (size_t)ntraj * B->ld);
+  L.dotpart = take(sizeof(double) * (size_t)ntraj * dot_blocks);
+  L.dotcount = take(sizeof(unsigned) * ntraj);
+  L.times = take(sizeof(double) * ntimes);
+  L.sysof = take(sizeof(int) * ntraj);
+  L.nof = take(sizeof(long long) * ntraj);
+  L.active = take(sizeof(int));
+  L.total = pos;
+  return L;
+}
+
+static void record_step(rpm_batch* Bh, const BatchDev& B, const Layout& L, cudaStream_t st) {
+  char* base = static_cast<char*>(Bh->buf);
+  const int m = B.m;
+  dim3 ew(B.nblk, B.ntraj);
+  k_b_start<<<ew, kEwThreads, 0, st>>>(B);
+  HpsiArgs<float2> a{};
+  a.ld = (long long)(m + 1) * B.ld;
+  a.ya_ld = B.ld;
+  a.in_scale = &B.st[0].scale;
+  a.scale_stride = kStateDoubles;
+  a.skip = &B.st[0].skip;
+  a.skip_stride = kStateInts;
+  a.views = Bh->views_dev;
+  a.sys_of = reinterpret_cast<const int*>(base + L.sysof);
+  a.dot_stride = kStateDoubles;
+  a.dot_part = reinterpret_cast<double*>(base + L.dotpart);
+  a.dot_count = reinterpret_cast<unsigned*>(base + L.dotcount);
+  float2* ya = reinterpret_cast<float2*>(base + L.ya);
+  for (int j = 0; j < m; ++j) {
+    a.in = B.V + (size_t)j * B.ld;
+    a.out = B.V + (size_t)(j + 1) * B.ld;
+    a.dot_out = &B.st[0].alpha[j];
+    launch_cube<float2>(a, Bh->plan, ya, B.ntraj, st);
+    k_b_update<<<ew, kEwThreads, 0, st>>>(B, j);
+  }
+  const size_t ctl_smem = sizeof(double) * 2 * kRecDoubles;
+  k_b_control<<<B.ntraj, 128, ctl_smem, st>>>(B);
+  k_b_rebuild<<<ew, kEwThreads, 0, st>>>(B);
+  k_b_gram<<<dim3(B.gblk, B.ntraj), 256, 0, st>>>(B);
+  k_b_observe<<<B.ntraj, 256, sizeof(double2) * kBMaxK * kBMaxK, st>>>(B);
+  check_launch("batched step");
+}
+
+static void run_batch(rpm_batch* Bh, int ntraj, const int* sys_of, void* psi, const double* times_host, int ntimes,
+                      double* values, double* errs, rpm_batch_stats* stats, cudaStream_t caller) {
+  const rpm_batch_config& cfg = Bh->cfg;
+  cudaStream_t st = Bh->work;
+  check_cuda(cudaEventRecord(Bh->ev_in, caller), "record entry event");
+  check_cuda(cudaStreamWaitEvent(st, Bh->ev_in, 0), "wait entry event");
+  if (ntraj < 1 || ntimes < 1) fail(RPM_E_INVALID, "At least one trajectory and one observation time are required.");
+  for (int k = 0; k < ntimes; ++k) {
+    if (!(times_host[k] >= 0.0) || (k && !(times_host[k] > times_host[k - 1])))
+      fail(RPM_E_INVALID, "Observation times must be nonnegative and strictly increasing.");
+  }
+  std::vector<long long> n_of(ntraj);
+  for (int b = 0; b < ntraj; ++b) {
+    if (sys_of[b] < 0 || sys_of[b] >= (int)Bh->systems.size()) fail(RPM_E_INVALID, "system index out of range");
+    n_of[b] = Bh->systems[sys_of[b]]->n;
+  }
+  const int nblk = (int)((Bh->ld + kEwChunk - 1) / kEwChunk);
+  const int gblk = std::max(1, std::min(32, (int)((Bh->ld / 4 + kGramChunk - 1) / kGramChunk)));
+  const int dot_blocks = std::max(Bh->plan.nl, 1);  // pass R grid.x <= nl
+  const Layout L = layout(Bh, ntraj, ntimes, nblk, gblk, dot_blocks);
+  if (L.total > Bh->buf_bytes) {
+    free_graph(Bh);
+    if (Bh->buf) check_cuda(cudaFree(Bh->buf), "cudaFree(batch)");
+    Bh->buf = nullptr;
+    check_cuda(cudaMalloc(&Bh->buf, L.total), "cudaMalloc(batch)");
+    Bh->buf_bytes = L.total;
+  }
+  char* base = static_cast<char*>(Bh->buf);
+  check_cuda(cudaMemsetAsync(base + L.count, 0, sizeof(unsigned) * ntraj, st), "memset counters");
+  check_cuda(cudaMemsetAsync(base + L.dotcount, 0, sizeof(unsigned) * ntraj, st), "memset counters");
+  check_cuda(cudaMemcpyAsync(base + L.times, times_host, sizeof(double) * ntimes, cudaMemcpyHostToDevice, st), "times");
+  check_cuda(cudaMemcpyAsync(base + L.sysof, sys_of, sizeof(int) * ntraj, cudaMemcpyHostToDevice, st), "sys_of");
+  check_cuda(cudaMemcpyAsync(base + L.nof, n_of.data(), sizeof(long long) * ntraj, cudaMemcpyHostToDevice, st), "n_of");
+  check_cuda(cudaMemcpyAsync(base + L.active, &ntraj, sizeof(int), cudaMemcpyHostToDevice, st), "active");
+
+  BatchDev B{};
+  B.st = reinterpret_cast<TrajState*>(base + L.st);
+  B.ntraj = ntraj;
+  B.m = cfg.krylov_dim;
+  B.offset = cfg.embedded_offset;
+  B.safety = cfg.safety_factor;
+  B.budget = cfg.state_error_budget;
+  B.max_step = cfg.maximum_step_us;
+  B.min_step = cfg.minimum_step_us;
+  B.t_end = times_host[ntimes - 1];
+  B.breakdown_rel = cfg.breakdown_relative;
+  B.times = reinterpret_cast<const double*>(base + L.times);
+  B.ntimes = ntimes;
+  B.ld = Bh->ld;
+  B.V = reinterpret_cast<float2*>(base + L.V);
+  B.psi = static_cast<double2*>(psi);
+  B.coef = reinterpret_cast<double2*>(base + L.coef);
+  B.perr = reinterpret_cast<double*>(base + L.perr);
+  B.part = reinterpret_cast<double*>(base + L.part);
+  B.count = reinterpret_cast<unsigned*>(base + L.count);
+  B.gpart = reinterpret_cast<double2*>(base + L.gpart);
+  B.values = values;
+  B.errs = errs;
+  B.nblk = nblk;
+  B.gblk = gblk;
+  B.active = reinterpret_cast<int*>(base + L.active);
+
+  k_b_setup<<<(ntraj + 127) / 128, 128, 0, st>>>(B, reinterpret_cast<const int*>(base + L.sysof),
+                                                 reinterpret_cast<const long long*>(base + L.nof),
+                                                 cfg.initial_step_us);
+  k_b_init<<<dim3(nblk, ntraj), kEwThreads, 0, st>>>(B);
+  check_launch("batched init");
+  const size_t ctl_smem = sizeof(double) * 2 * kRecDoubles;
+  check_cuda(cudaFuncSetAttribute(k_b_control, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctl_smem),
+             "control attr");
+  check_cuda(cudaFuncSetAttribute(k_b_observe, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(sizeof(double2) * kBMaxK * kBMaxK)),
+             "observe attr");
+
+  const bool use_graph = cfg.use_graph != 0;
+  if (use_graph) {
+    // one eager step sets every kernel attribute before capture
+    record_step(Bh, B, L, st);
+    free_graph(Bh);
+    check_cuda(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+    record_step(Bh, B, L, st);
+    check_cuda(cudaStreamEndCapture(st, &Bh->graph), "end capture");
+    check_cuda(cudaGraphInstantiate(&Bh->exec, Bh->graph, 0), "graph instantiate");
+  }
+  int active = ntraj;
+  long long replays = 0;
+  const long long max_replays = cfg.max_steps > 0 ? cfg.max_steps : 10000000LL;
+  while (active > 0) {
+    for (int r = 0; r < 4; ++r) {
+      if (use_graph) check_cuda(cudaGraphLaunch(Bh->exec, st), "graph launch");
+      else record_step(Bh, B, L, st);
+      ++replays;
+    }
+    check_cuda(cudaMemcpyAsync(&active, base + L.active, sizeof(int), cudaMemcpyDeviceToHost, st), "poll");
+    check_cuda(cudaStreamSynchronize(st), "poll sync");
+    if (replays > max_replays) fail(RPM_E_NUMERIC, "batched propagation exceeded the step limit");
+  }
+  std::vector<TrajState> host(ntraj);
+  check_cuda(cudaMemcpyAsync(host.data(), B.st, sizeof(TrajState) * ntraj, cudaMemcpyDeviceToHost, st), "stats");
+  check_cuda(cudaStreamSynchronize(st), "stats sync");
+  check_cuda(cudaEventRecord(Bh->ev_out, st), "record exit event");
+  check_cuda(cudaStreamWaitEvent(caller, Bh->ev_out, 0), "wait exit event");
+  for (int b = 0; b < ntraj; ++b) {
+    rpm_batch_stats& o = stats[b];
+    o.accepted_steps = host[b].steps;
+    o.rejected_steps = 0;
+    o.matvecs = host[b].matvecs;
+    o.maximum_krylov_dimension = cfg.krylov_dim;
+    o.minimum_step_us = host[b].steps ? host[b].min_step : 0.0;
+    o.maximum_step_us = host[b].max_step;
+    o.accumulated_state_error = host[b].acc_err;
+    o.maximum_norm_error = host[b].max_norm_err;
+    o.status = host[b].status;
+  }
+}
+
+}  // namespace rpm
+
+using namespace rpm;
+
+extern "C" {
+
+int rpm_batch_create(rpm_system* const* systems, int nsys, const rpm_batch_config* cfg, rpm_batch** out) {
+  return guarded([&] {
+    if (!out || !systems || nsys < 1 || !cfg) fail(RPM_E_INVALID, "bad arguments");
+    *out = nullptr;
+    if (cfg->krylov_dim < 2 || cfg->krylov_dim > kBMaxK) fail(RPM_E_UNSUPPORTED, "batched Krylov dimension must be in [2, 64]");
+    if (cfg->embedded_offset < 1 || cfg->embedded_offset >= cfg->krylov_dim)
+      fail(RPM_E_INVALID, "embedded offset must be in [1, krylov_dim)");
+    if (!(cfg->state_error_budget > 0.0) || !(cfg->maximum_step_us > 0.0)) fail(RPM_E_INVALID, "bad step controls");
+    auto B = std::make_unique<rpm_batch>();
+    B->cfg = *cfg;
+    std::vector<CubeView<float2>> views;
+    for (int k = 0; k < nsys; ++k) {
+      rpm_system* s = systems[k];
+      if (!s || !s->on_device) fail(RPM_E_INVALID, "every system must be on the device");
+      if (!s->cube) fail(RPM_E_UNSUPPORTED, "the batched path needs the radical-split cube form");
+      if (s->ndims < 2 || s->dims[0] != 2 || s->dims[1] != 2)
+        fail(RPM_E_INVALID, "The first two axes must be the two electron spins.");
+      B->systems.push_back(s);
+      views.push_back(s->cube32);
+      B->ld = std::max(B->ld, s->n);
+    }
+    B->ld = (B->ld + 63) & ~63LL;
+    B->plan = cube_plan(B->systems.data(), nsys);
+    check_cuda(cudaStreamCreateWithFlags(&B->work, cudaStreamNonBlocking), "create batch stream");
+    check_cuda(cudaEventCreateWithFlags(&B->ev_in, cudaEventDisableTiming), "create event");
+    check_cuda(cudaEventCreateWithFlags(&B->ev_out, cudaEventDisableTiming), "create event");
+    check_cuda(cudaMalloc(&B->views_dev, sizeof(CubeView<float2>) * nsys), "cudaMalloc(views)");
+    check_cuda(cudaMemcpy(B->views_dev, views.data(), sizeof(CubeView<float2>) * nsys, cudaMemcpyHostToDevice),
+               "copy views");
+    *out = B.release();
+  });
+}
+
+int rpm_batch_leading_dimension(const rpm_batch* batch, long long* ld) {
+  return guarded([&] {
+    if (!batch || !ld) fail(RPM_E_INVALID, "bad arguments");
+    *ld = batch->ld;
+  });
+}
+
+int rpm_batch_propagate(rpm_batch* batch, int ntraj, const int* sys_of_host, void* psi_dev, const double* times_host,
+                        int ntimes, double* values_dev, double* state_errors_dev, rpm_batch_stats* stats_host,
+                        void* stream) {
+  return guarded([&] {
+    if (!batch || !sys_of_host || !psi_dev || !times_host || !values_dev || !state_errors_dev || !stats_host)
+      fail(RPM_E_INVALID, "NULL argument");
+    run_batch(batch, ntraj, sys_of_host, psi_dev, times_host, ntimes, values_dev, state_errors_dev, stats_host,
+              static_cast<cudaStream_t>(stream));
+  });
+}
+
+int rpm_batch_destroy(rpm_batch* batch) {
+  return guarded([&] {
+    if (!batch) return;
+    free_graph(batch);
+    if (batch->work) cudaStreamSynchronize(batch->work);
+    if (batch->buf) cudaFree(batch->buf);
+    if (batch->views_dev) cudaFree(batch->views_dev);
+    if (batch->ev_in) cudaEventDestroy(batch->ev_in);
+    if (batch->ev_out) cudaEventDestroy(batch->ev_out);
+    if (batch->work) cudaStreamDestroy(batch->work);
+    delete batch;
+  });
+}
+
+}  // extern "C"

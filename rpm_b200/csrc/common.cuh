@@ -140,6 +140,46 @@ struct GenericView {
   const int* coloff;  // for each term: memory offset of local column c relative to the row-zero base
 };
 
+// ---------------------------------------------------------------------------
+// "Cube" form of one radical group (see hpsi.cu).  The group index is
+//   g = e * half + sum_k n_k * gs[k]      (e: electron digit, n_k: nuclei)
+// and every group term acts on {e}, {n_k} or {e, n_k}.  Per nucleus k the
+// combined 2d x 2d block O_k on (e, n_k) is split into
+//   D_k[e][m]            = Re O_k[(e,m),(e,m)]          (merged diagonal)
+//   F_k[e][m]            = O_k[(e,m),(1-e,m)]           (merged electron flip)
+//   X_k[(e,m),(e',m')]   = O_k[(e,m),(e',m')], m' != m  (nuclear transitions)
+// The electron-only operator Z adds Zd[e] = Re Z[e][e] and Zf[e] = Z[e][1-e].
+// Table layout (complex entries): [Zd0, Zd1, Zf0, Zf1], then per nucleus
+// D (2d), F (2d), X ((2d)^2) at offD/offF/offX.
+// ---------------------------------------------------------------------------
+constexpr int kCubeMaxDigits = 16;
+constexpr int kCubeMaxTable = 2048;
+
+struct CubeSide {
+  int K;        // nuclear digits in the group
+  int half;     // group size / 2 (electron stride)
+  int n_outer;  // product of the dims of the outer digits (all but the last NI)
+  int ntab;     // table length in complex entries
+  int dim[kCubeMaxDigits];
+  int gs[kCubeMaxDigits];
+  int offD[kCubeMaxDigits], offF[kCubeMaxDigits], offX[kCubeMaxDigits];
+};
+
+// Coefficient storage of the cube tables (same precision as the state).
+template <class T> struct CubeCoef { using type = T; };
+
+template <class T>
+struct CubeView {
+  CubeSide L, R;
+  const typename CubeCoef<T>::type* tabL;
+  const typename CubeCoef<T>::type* tabR;
+  T pair[16];  // (a b) x (a' b') electron-pair operator
+  const int* offl;
+  const int* offr;
+  int nl, nr, half_l, half_r;
+  int inner_l, inner_r;  // usable trailing spin-1/2 digits per side
+};
+
 }  // namespace rpm
 
 // The opaque system object of the C ABI.
@@ -166,6 +206,14 @@ struct rpm_system {
   rpm::SplitView<float2> split32{};
   rpm::GenericView<double2> gen64{};
   rpm::GenericView<float2> gen32{};
+  // cube form (valid when `cube` is true)
+  bool cube = false;
+  rpm::CubeSide cube_l{}, cube_r{};
+  std::vector<rpm::cd> cube_tab_l, cube_tab_r;
+  rpm::CubeView<double2> cube64{};
+  rpm::CubeView<float2> cube32{};
+  rpm::CubeView<double2>* cube64_dev = nullptr;  // device copy of cube64
+  rpm::CubeView<float2>* cube32_dev = nullptr;
   std::vector<void*> allocations;
 
   // scratch buffers, one per slot, grown on demand (cudaMalloc'd) ---------

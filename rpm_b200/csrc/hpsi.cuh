@@ -1,0 +1,42 @@
+// Launch interface of the H psi kernels (hpsi.cu), shared with batched.cu.
+#pragma once
+
+#include "common.cuh"
+
+namespace rpm {
+
+// Arguments of one batched H psi launch.  Vector b of the batch is read from
+// in + b*ld and written to out + b*ld; everything else is optional.
+template <class T>
+struct HpsiArgs {
+  const T* in;
+  T* out;
+  long long ld;
+  long long ya_ld;  // stride of the pass-L scratch per vector (0: same as ld)
+  const double* in_scale;  // input multiplier of vector b at in_scale[b*scale_stride]
+  int scale_stride;
+  const int* skip;         // vector b untouched when skip[b*skip_stride] != 0
+  int skip_stride;
+  const CubeView<T>* views;  // device array of system views
+  const int* sys_of;         // view index of vector b (NULL: view 0)
+  // fused <in_scaled, H in_scaled> of vector b into dot_out[b*dot_stride]
+  double* dot_out;
+  int dot_stride;
+  double* dot_part;     // gridDim.x partials per vector
+  unsigned* dot_count;  // one completion counter per vector (zero on entry)
+};
+
+// Shape limits of one launch over one or more systems.
+struct CubePlan {
+  int nl, nr, half_r, tab_cap;
+  int ni_l, ni_r;  // inner digits used per side
+  int n_outer_l1, n_outer_l2, n_outer_r1, n_outer_r2;  // outer-index counts for NI = 1, 2
+};
+
+int sm_count();
+CubePlan cube_plan(rpm_system* const* systems, int nsys);
+// Two passes: pass L into `ya` (batch x ld scratch), pass R into a.out.
+template <class T>
+void launch_cube(const HpsiArgs<T>& a, const CubePlan& p, T* ya, int batch, cudaStream_t stream);
+
+}  // namespace rpm

@@ -146,10 +146,13 @@ static __device__ int tridiag_qr(int m, double* d, double* e, double* z, int ldz
 }
 
 // c = exp(-i T t) e1 from a spectra record, into shared `c` (m entries).
+// Record layout with leading dimension LD: [0] size, [1] status, [2, 2+LD)
+// eigenvalues, then LD x LD eigenvectors (row i = component i).
+template <int LD = RPM_MAX_KRYLOV>
 static __device__ void spectral_coefficients(const double* rec, double t, double2* ph, double2* c) {
   const int m = (int)rec[0];
   const double* lam = rec + 2;
-  const double* z = rec + 2 + RPM_MAX_KRYLOV;
+  const double* z = rec + 2 + LD;
   for (int k = threadIdx.x; k < m; k += blockDim.x) {
     double s, co;
     sincos(lam[k] * t, &s, &co);
@@ -158,7 +161,7 @@ static __device__ void spectral_coefficients(const double* rec, double t, double
   }
   __syncthreads();
   for (int i = threadIdx.x; i < m; i += blockDim.x) {
-    const double* zi = z + i * RPM_MAX_KRYLOV;
+    const double* zi = z + i * LD;
     double2 acc = make_double2(0.0, 0.0);
     for (int k = 0; k < m; ++k) {
       acc.x = fma(zi[k], ph[k].x, acc.x);

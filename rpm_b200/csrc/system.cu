@@ -118,6 +118,71 @@ static void build_group_csr(const std::vector<int>& gdims, const std::vector<Gro
   }
 }
 
+// Cube tables of one radical group (see CubeSide in common.cuh).  Returns
+// false when a group term acts on anything but {e}, {n_k} or {e, n_k}.
+static bool build_cube_side(const std::vector<int>& gdims, const std::vector<GroupTerm>& gterms, CubeSide& side,
+                            std::vector<cd>& tab, int& inner) {
+  const int K = (int)gdims.size() - 1;
+  if (K < 1 || K > kCubeMaxDigits || gdims[0] != 2) return false;
+  side = CubeSide{};
+  side.K = K;
+  long long stride = 1;
+  for (int k = K - 1; k >= 0; --k) {
+    side.dim[k] = gdims[k + 1];
+    side.gs[k] = (int)stride;
+    stride *= gdims[k + 1];
+  }
+  side.half = (int)stride;
+  cd Z[2][2] = {};
+  std::vector<std::vector<cd>> O(K);
+  for (int k = 0; k < K; ++k) O[k].assign((size_t)4 * side.dim[k] * side.dim[k], 0.0);
+  for (const GroupTerm& t : gterms) {
+    if (t.pos.size() == 1 && t.pos[0] == 0) {
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) Z[a][b] += t.op[a * 2 + b];
+    } else if (t.pos.size() == 1) {
+      const int k = t.pos[0] - 1, d = side.dim[k];
+      for (int e = 0; e < 2; ++e)
+        for (int m = 0; m < d; ++m)
+          for (int mp = 0; mp < d; ++mp) O[k][(size_t)(e * d + m) * 2 * d + e * d + mp] += t.op[m * d + mp];
+    } else if (t.pos.size() == 2 && (t.pos[0] == 0 || t.pos[1] == 0)) {
+      const bool e_first = t.pos[0] == 0;
+      const int k = (e_first ? t.pos[1] : t.pos[0]) - 1, d = side.dim[k];
+      for (int e = 0; e < 2; ++e)
+        for (int m = 0; m < d; ++m)
+          for (int ep = 0; ep < 2; ++ep)
+            for (int mp = 0; mp < d; ++mp) {
+              const int row = e_first ? e * d + m : m * 2 + e;
+              const int col = e_first ? ep * d + mp : mp * 2 + ep;
+              O[k][(size_t)(e * d + m) * 2 * d + ep * d + mp] += t.op[(size_t)row * 2 * d + col];
+            }
+    } else {
+      return false;
+    }
+  }
+  tab.assign(4, 0.0);
+  tab[0] = Z[0][0].real();
+  tab[1] = Z[1][1].real();
+  tab[2] = Z[0][1];
+  tab[3] = Z[1][0];
+  for (int k = 0; k < K; ++k) {
+    const int d = side.dim[k];
+    side.offD[k] = (int)tab.size();
+    for (int e = 0; e < 2; ++e)
+      for (int m = 0; m < d; ++m) tab.push_back(O[k][(size_t)(e * d + m) * 2 * d + e * d + m].real());
+    side.offF[k] = (int)tab.size();
+    for (int e = 0; e < 2; ++e)
+      for (int m = 0; m < d; ++m) tab.push_back(O[k][(size_t)(e * d + m) * 2 * d + (1 - e) * d + m]);
+    side.offX[k] = (int)tab.size();
+    tab.insert(tab.end(), O[k].begin(), O[k].end());
+  }
+  side.ntab = (int)tab.size();
+  if (side.ntab > kCubeMaxTable) return false;
+  inner = 0;
+  while (inner < K && side.dim[K - 1 - inner] == 2) ++inner;
+  return true;
+}
+
 template <class T>
 static T* upload(rpm_system* sys, const void* src, size_t bytes) {
   void* p = nullptr;
@@ -184,6 +249,30 @@ static void upload_system(rpm_system* sys) {
     }
     sys->split64 = s64;
     sys->split32 = s32;
+    if (sys->cube) {
+      auto tl64 = to_d2(sys->cube_tab_l), tr64 = to_d2(sys->cube_tab_r);
+      auto tl32 = to_f2(sys->cube_tab_l), tr32 = to_f2(sys->cube_tab_r);
+      CubeView<double2>& c64 = sys->cube64;
+      CubeView<float2>& c32 = sys->cube32;
+      c64.L = c32.L = sys->cube_l;
+      c64.R = c32.R = sys->cube_r;
+      c64.tabL = upload<double2>(sys, tl64.data(), tl64.size() * sizeof(double2));
+      c64.tabR = upload<double2>(sys, tr64.data(), tr64.size() * sizeof(double2));
+      c32.tabL = upload<float2>(sys, tl32.data(), tl32.size() * sizeof(float2));
+      c32.tabR = upload<float2>(sys, tr32.data(), tr32.size() * sizeof(float2));
+      for (int k = 0; k < 16; ++k) {
+        c64.pair[k] = s64.pair[k];
+        c32.pair[k] = s32.pair[k];
+      }
+      c64.offl = c32.offl = d_offl;
+      c64.offr = c32.offr = d_offr;
+      c64.nl = c32.nl = sys->nl;
+      c64.nr = c32.nr = sys->nr;
+      c64.half_l = c32.half_l = sys->half_l;
+      c64.half_r = c32.half_r = sys->half_r;
+      sys->cube64_dev = upload<CubeView<double2>>(sys, &c64, sizeof(c64));
+      sys->cube32_dev = upload<CubeView<float2>>(sys, &c32, sizeof(c32));
+    }
   }
   sys->on_device = true;
 }
@@ -307,6 +396,11 @@ static rpm_system* create_system(const int* dims, int ndims, const rpm_term* ter
     for (int a : rg) rdims.push_back(dims[a]);
     build_group_csr(ldims, lterms, sys->lptr, sys->lcol, sys->lval);
     build_group_csr(rdims, rterms, sys->rptr, sys->rcol, sys->rval);
+    int inner_l = 0, inner_r = 0;
+    sys->cube = build_cube_side(ldims, lterms, sys->cube_l, sys->cube_tab_l, inner_l) &&
+                build_cube_side(rdims, rterms, sys->cube_r, sys->cube_tab_r, inner_r);
+    sys->cube64.inner_l = sys->cube32.inner_l = inner_l;
+    sys->cube64.inner_r = sys->cube32.inner_r = inner_r;
     auto offsets = [&](const std::vector<int>& g, const std::vector<int>& gd) {
       long long size = 1;
       for (int v : gd) size *= v;
