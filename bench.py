@@ -1,0 +1,414 @@
+"""Benchmark: radical-pair trajectories/s at 221,184 dimensions.
+
+Default arm (``--impl b200``): the batched mixed-precision GPU path over the
+full-size FAD-TrpH-shaped synthetic radical pair, 12 Fibonacci-sphere field
+orientations x V random-phase vectors per step, propagated to 5 us on the
+0.00125-us grid with the singlet yield (tau = 1 us).  One "step" is one such
+batch.  ``value`` is whole-job trajectories/s with the states resident in HBM;
+``e2e`` is the same through the public Python API from pinned host buffers.
+Beside it: the plain single-vector FP64 GPU path on one trajectory (the
+reference's controller, Krylov 8-40, budget 1e-10) and the yield error of the
+batched path against it, the H psi roofline, and the CPU baseline (the
+oracle's NumPy/SciPy port of the reference's FP64 path on all host cores, on a
+bounded prefix of the horizon).
+
+Reference arm (``--impl reference``): that CPU port alone, on the host cores.
+
+Multi-GPU (torchrun): every rank propagates its own batch (weak scaling, no
+data-path collective); per-trajectory yields are all-gathered at the end.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+METRIC = "RP trajectories/s at 221,184-dim, batched vs plain GPU, yield err ≤1e-6"
+UNIT = "trajectories/s"
+HORIZON_US = 5.0
+GRID_US = 0.00125
+LIFETIME_US = 1.0
+FALLBACK_HBM_GBS = 6650.0
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline (oracle port), run in spawned worker processes
+# ---------------------------------------------------------------------------
+_CPU_STATE = {}
+
+
+def _cpu_worker_init():
+    import oracle
+    from rpm_b200 import synthetic
+
+    full = synthetic.full_system()
+    terms = full.terms(math.pi / 4, 0.0)
+    h = oracle.CompiledFullPairHamiltonian(full.dimensions, [oracle.LocalTerm(t.axes, t.operator) for t in terms],
+                                           left_axes=full.left_axes, right_axes=full.right_axes)
+    _CPU_STATE["h"] = h
+    _CPU_STATE["dims"] = full.dimensions
+
+
+def _cpu_worker_run(args):
+    seed, horizon = args
+    import numpy as np
+
+    import oracle
+    from rpm_b200 import synthetic
+
+    h = _CPU_STATE["h"]
+    psi = synthetic.random_phase_vectors(_CPU_STATE["dims"], 1, seed)[0]
+    times = np.arange(int(round(horizon / GRID_US)) + 1) * GRID_US
+    prop = oracle.AdaptiveLanczosPropagator(h, minimum_dimension=8, maximum_dimension=40,
+                                            state_error_budget=1e-10 * horizon / HORIZON_US)
+    t0 = time.perf_counter()
+    res = prop.propagate(psi, times, oracle.SingletPopulationObservable(_CPU_STATE["dims"]))
+    return time.perf_counter() - t0, res.stats.matvecs
+
+
+class CpuBaseline:
+    """The oracle's FP64 port on `workers` host processes (one BLAS thread each)."""
+
+    def __init__(self, workers: int):
+        import multiprocessing as mp
+
+        for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+            os.environ[var] = "1"
+        self.workers = workers
+        self.pool = mp.get_context("spawn").Pool(workers, initializer=_cpu_worker_init)
+
+    def round(self, horizon: float, seed0: int):
+        """One round: every worker propagates one trajectory over `horizon` us."""
+        t0 = time.perf_counter()
+        out = self.pool.map(_cpu_worker_run, [(seed0 + k, horizon) for k in range(self.workers)])
+        wall = time.perf_counter() - t0
+        per_traj = sum(o[0] for o in out) / len(out)
+        # trajectories/s over the full horizon, all workers in parallel
+        return self.workers / (wall * HORIZON_US / horizon), per_traj, wall
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
+def cpu_workers() -> int:
+    n = os.cpu_count() or 1
+    return max(1, min(n, 64))
+
+
+# ---------------------------------------------------------------------------
+# Clock sampling during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_uuid: str | None):
+        self.proc = None
+        self.lines: list[str] = []
+        try:
+            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+            if device_uuid:
+                cmd += ["-i", device_uuid]
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = max(smax, float(parts[1]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[3:7]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    path = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(path.read_text())["hbm_gbs"]), "measured"
+    except (OSError, ValueError, KeyError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic_per_vector():
+    """DRAM bytes per vector of one batched H psi (both passes) from the
+    committed ncu summary, or None."""
+    path = ROOT / "profiles" / "hpsi_cube_c64_batched.md"
+    try:
+        for line in path.read_text().splitlines():
+            if line.startswith("dram_bytes_per_vector:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+# Arms
+# ---------------------------------------------------------------------------
+def reference_arm(args, rank: int, world: int) -> None:
+    if rank != 0:
+        return
+    base = CpuBaseline(cpu_workers())
+    horizon = args.cpu_horizon
+    for k in range(args.warmup):
+        base.round(horizon, 1000 + 64 * k)
+    vals = []
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        v, _, _ = base.round(horizon, 5000 + 64 * k)
+        vals.append(v)
+    wall = time.perf_counter() - t0
+    base.close()
+    value = sum(vals) / len(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * wall / max(1, args.steps), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {"workload": "plain FP64 Lanczos (Krylov 8-40, budget 1e-10) on the 221,184-dim synthetic "
+                               "radical pair, theta = pi/4, one trajectory per host core, extrapolated from a "
+                               f"{horizon} us prefix to 5 us"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": base.workers, "kind": "port",
+                         "sample": f"each step: {base.workers} trajectories x {horizon} us prefix, extrapolated"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def b200_arm(args, rank: int, world: int, dist) -> None:
+    import numpy as np
+    import torch
+
+    import rpm_b200 as rb
+    from rpm_b200 import synthetic
+    from rpm_b200.batched import BatchedPropagator
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    full = synthetic.full_system()
+    dirs = synthetic.fibonacci_sphere(args.orientations)
+    hams = [rb.CompiledFullPairHamiltonian(full.dimensions, full.terms(th, ph), left_axes=full.left_axes,
+                                           right_axes=full.right_axes) for th, ph in dirs]
+    n = full.dimension
+    nvec = args.vectors
+    ntraj = args.orientations * nvec
+    seed = 1000 + rank
+    vecs = synthetic.random_phase_vectors(full.dimensions, nvec, seed)
+    states = np.stack([vecs[v] for k in range(args.orientations) for v in range(nvec)])
+    system_index = np.array([k for k in range(args.orientations) for _ in range(nvec)], dtype=np.int32)
+    times = np.arange(int(round(HORIZON_US / GRID_US)) + 1) * GRID_US
+    bp = BatchedPropagator(hams, krylov_dimension=args.krylov, state_error_budget=args.budget)
+    ld = bp.leading_dimension
+    pristine = torch.zeros((ntraj, ld), dtype=torch.complex128, device=dev)
+    pristine[:, :n].copy_(torch.from_numpy(states))
+    work = torch.empty_like(pristine)
+
+    def step():
+        work.copy_(pristine)
+        values, _, stats = bp.propagate_device(work, times, system_index)
+        return values, stats
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    bp.counters(reset=True)
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    clocks = ClockSampler(uuid)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t_start.record()
+    values = stats = None
+    for _ in range(args.steps):
+        values, stats = step()
+    t_end.record()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clock_info = clocks.stop()
+    elapsed = t_start.elapsed_time(t_end) / 1e3
+    if dist is not None:
+        t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    counters = bp.counters(reset=True)
+    value = args.steps * ntraj * world / elapsed
+    yields = bp.yields_device(times, values, LIFETIME_US)
+    if dist is not None:
+        gathered = torch.empty(world * ntraj, dtype=torch.float64, device=dev)
+        dist.all_gather_into_tensor(gathered, yields)
+        yields_all = gathered
+    else:
+        yields_all = yields
+    bad = [s.status for s in stats if s.status]
+    if bad:
+        raise RuntimeError(f"batched propagation failed with status {bad[0]}")
+
+    # end-to-end through the public API from pinned host memory
+    host_states = torch.from_numpy(states).pin_memory()
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(e2e_steps):
+        res = bp.propagate(host_states, times, system_index=system_index, lifetime_us=LIFETIME_US)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_elapsed = e0.elapsed_time(e1) / 1e3
+    if dist is not None:
+        t = torch.tensor([e2e_elapsed], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_elapsed = float(t.item())
+    e2e_value = e2e_steps * ntraj * world / e2e_elapsed
+    h2d = ntraj * n * 16
+    d2h = res.observable_values.nbytes + res.state_error_estimates.nbytes + res.yields.nbytes
+
+    line = None
+    if rank == 0:
+        # roofline of the dominant kernel: one batched H psi (pass L + pass R)
+        peak, peak_src = measured_peak_hbm()
+        hpsi_s = counters["hpsi_ms"] / 1e3
+        alg_bytes = 16.0 * n * ntraj
+        achieved = alg_bytes / hpsi_s / 1e9 if hpsi_s > 0 else None
+        per_vec = ncu_traffic_per_vector()
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak if achieved else None,
+                    "traffic": per_vec * ntraj if per_vec is not None else None,
+                    "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured" else "fallback",
+                    "kernel": "cube_pass_l + cube_pass_r (complex64 H psi, one batched launch pair)",
+                    "algorithmic_bytes": alg_bytes, "avg_launch_ms": counters["hpsi_ms"],
+                    "samples": counters["hpsi_samples"]}
+        # plain single-vector FP64 GPU path on trajectory 0 (same state and system)
+        plain, y_err = None, None
+        if not args.no_plain:
+            t0 = time.perf_counter()
+            ref = rb.AdaptiveLanczosPropagator(hams[0], minimum_dimension=8, maximum_dimension=40,
+                                               state_error_budget=1e-10).propagate(
+                states[0], times, rb.SingletPopulationObservable(full.dimensions))
+            torch.cuda.synchronize()
+            plain_s = time.perf_counter() - t0
+            y_plain = rb.integrate_yield(times, ref.observable_values, LIFETIME_US)
+            y_err = abs(float(yields[0].item()) - y_plain)
+            plain = {"value": 1.0 / plain_s, "unit": UNIT, "sample": "1 trajectory (orientation 0, vector 0), 5 us",
+                     "matvecs": ref.stats.matvecs, "krylov": "8-40", "budget": 1e-10}
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            base = CpuBaseline(cpu_workers())
+            cpu_value, per_traj, wall = base.round(args.cpu_horizon, 77)
+            base.close()
+            cpu = {"value": cpu_value, "unit": UNIT, "cores": base.workers, "kind": "port",
+                   "sample": f"{base.workers} trajectories x {args.cpu_horizon} us prefix (Krylov 8-40, budget "
+                             f"1e-10 scaled), extrapolated to 5 us; {per_traj:.1f} s each"}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64 H-psi/basis + f64 Krylov control", "data": "synthetic",
+            "config": {"workload": f"batched mixed-precision propagation, 221,184-dim synthetic FAD-TrpH-shaped radical "
+                                   f"pair (2 e + 11 spin-1/2 + 3 spin-1), {args.orientations} Fibonacci field "
+                                   f"orientations x {nvec} random-phase vectors per GPU per step, 5 us, "
+                                   f"0.00125-us grid (4001 points), singlet yield tau = 1 us",
+                       "trajectories_per_step_per_gpu": ntraj, "krylov_dim": args.krylov,
+                       "state_error_budget": args.budget, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (Krylov basis " f"{ntraj * (args.krylov + 1) * n * 8 / 1e9:.1f} GB)"},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps": e2e_steps},
+            "gpu_launches": counters["kernel_launches"],
+            "clocks": clock_info,
+            "plain_fp64": plain,
+            "batched_over_plain": value / world / plain["value"] if plain else None,
+            "yield_err_vs_fp64": y_err,
+            "yields_gathered": int(yields_all.numel()),
+        }
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    p = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=8)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    p.add_argument("--orientations", type=int, default=12)
+    p.add_argument("--vectors", type=int, default=4, help="random-phase vectors per orientation per GPU")
+    p.add_argument("--krylov", type=int, default=32)
+    p.add_argument("--budget", type=float, default=1e-7)
+    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--cpu-horizon", type=float, default=0.025, help="us of the CPU baseline sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison trajectory")
+    args = p.parse_args()
+    if args.warmup < 0 or args.steps < 1:
+        raise SystemExit("steps must be >= 1 and warmup >= 0")
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist_mod
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        backend = "nccl" if args.impl == "b200" else "gloo"
+        dist_mod.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        dist = dist_mod
+    try:
+        if args.impl == "reference":
+            reference_arm(args, rank, world)
+        else:
+            b200_arm(args, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -192,6 +192,12 @@ int rpm_batch_leading_dimension(const rpm_batch* batch, long long* ld);
 int rpm_batch_propagate(rpm_batch* batch, int ntraj, const int* sys_of_host, void* psi_dev,
                         const double* times_host, int ntimes, double* values_dev,
                         double* state_errors_dev, rpm_batch_stats* stats_host, void* stream);
+/* Measurement counters since creation or the last reset: kernels launched,
+ * Krylov-step replays, and the mean duration (ms) of one batched H psi (both
+ * passes, all trajectories) sampled inside the graph while no trajectory had
+ * finished. */
+int rpm_batch_counters(rpm_batch* batch, int reset, long long* kernel_launches, long long* step_replays,
+                       double* hpsi_ms_mean, long long* hpsi_samples);
 int rpm_batch_destroy(rpm_batch* batch);
 
 #ifdef __cplusplus

@@ -284,8 +284,16 @@ class CompiledFullPairHamiltonian:
         self.right_dimensions = tuple(self.dimensions[a] for a in right)
         self.left_dimension = math.prod(self.left_dimensions)
         self.right_dimension = math.prod(self.right_dimensions)
-        self.left_operator = MatrixFreeHamiltonian(self.left_dimensions, lterms).explicit_matrix()
-        self.right_operator = MatrixFreeHamiltonian(self.right_dimensions, rterms).explicit_matrix()
+        # dense blocks assembled term by term, then held as CSR like the
+        # reference (scipy.sparse.csr_matrix + eliminate_zeros)
+        import scipy.sparse
+
+        left_dense = MatrixFreeHamiltonian(self.left_dimensions, lterms).explicit_matrix()
+        right_dense = MatrixFreeHamiltonian(self.right_dimensions, rterms).explicit_matrix()
+        self.left_operator = scipy.sparse.csr_matrix(left_dense)
+        self.right_operator = scipy.sparse.csr_matrix(right_dense)
+        self.left_operator.eliminate_zeros()
+        self.right_operator.eliminate_zeros()
         self.electron_pair_operator = pair.reshape(2, 2, 2, 2)
 
     def matvec(self, vector) -> np.ndarray:
@@ -294,7 +302,7 @@ class CompiledFullPairHamiltonian:
             raise ValueError(f"Vector length {flat.size} does not match {self.dimension}.")
         grouped = np.transpose(flat.reshape(self.dimensions), self.permutation)
         psi = grouped.reshape(self.left_dimension, self.right_dimension)
-        out = self.left_operator @ psi + psi @ self.right_operator.T
+        out = self.left_operator @ psi + (self.right_operator @ psi.T).T
         four = grouped.reshape(2, self.left_dimension // 2, 2, self.right_dimension // 2)
         out += np.einsum("abcd,cxdy->axby", self.electron_pair_operator, four).reshape(psi.shape)
         back = np.transpose(out.reshape(self.left_dimensions + self.right_dimensions), self.inverse_permutation)

@@ -94,6 +94,7 @@ SIGNATURES: dict[str, list] = {
     "rpm_batch_leading_dimension": [_P, _PLL],
     "rpm_batch_propagate": [_P, _I, _PI, _P, _PD, _I, _P, _P, ctypes.POINTER(rpm_batch_stats), _P],
     "rpm_batch_destroy": [_P],
+    "rpm_batch_counters": [_P, _I, _PLL, _PLL, _PD, _PLL],
 }
 
 _lib = None

@@ -102,9 +102,15 @@ class BatchedPropagator:
         idx = np.asarray(system_index, dtype=np.int32)
         ntraj = idx.size
         buf = torch.zeros((ntraj, self.leading_dimension), dtype=torch.complex128, device="cuda")
-        if isinstance(initial_states, torch.Tensor) and initial_states.ndim == 2 and \
-                initial_states.shape[1] == self.leading_dimension:
-            buf.copy_(initial_states)
+        sizes = {self.hamiltonians[k].dimension for k in idx}
+        if isinstance(initial_states, (torch.Tensor, np.ndarray)) and initial_states.ndim == 2 and len(sizes) == 1:
+            n = sizes.pop()
+            if initial_states.shape[1] < n:
+                raise ValueError("Initial state dimension does not match the Hamiltonian.")
+            src = initial_states if isinstance(initial_states, torch.Tensor) else torch.from_numpy(
+                np.ascontiguousarray(initial_states, dtype=np.complex128))
+            # one copy for the whole batch (asynchronous from pinned host memory)
+            buf[:, :n].copy_(src[:, :n], non_blocking=True)
             return buf
         for b in range(ntraj):
             n = self.hamiltonians[idx[b]].dimension
@@ -129,6 +135,14 @@ class BatchedPropagator:
         _lib.call("rpm_batch_propagate", self._handle, ntraj, _lib.iptr(idx), _lib.ptr(psi), _lib.dptr(times),
                   int(times.size), _lib.ptr(values), _lib.ptr(errs), stats, _lib.stream_handle(stream))
         return values, errs, stats
+
+    def counters(self, reset: bool = False) -> dict:
+        """Kernel launches, Krylov-step replays and the mean batched H psi time (ms)."""
+        k, r, n = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        ms = ctypes.c_double()
+        _lib.call("rpm_batch_counters", self._handle, 1 if reset else 0, ctypes.byref(k), ctypes.byref(r),
+                  ctypes.byref(ms), ctypes.byref(n))
+        return {"kernel_launches": k.value, "step_replays": r.value, "hpsi_ms": ms.value, "hpsi_samples": n.value}
 
     def yields_device(self, times_us, values, lifetime_us: float):
         """Simpson yields of each row of ``values`` on the GPU (FP64, compensated)."""

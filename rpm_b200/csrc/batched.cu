@@ -533,6 +533,14 @@ struct rpm_batch {
   // on entry and before it on exit through events.
   cudaStream_t work = nullptr;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  // Measurement: a timed event pair around the H psi of Lanczos iteration 1 of
+  // every Krylov step (recorded inside the graph), sampled at each poll while
+  // every trajectory is still running; and the number of kernels launched.
+  cudaEvent_t probe0 = nullptr, probe1 = nullptr;
+  double probe_ms_sum = 0.0;
+  long long probe_samples = 0;
+  long long kernel_launches = 0, replays = 0;
+  int launches_per_step = 0;
 };
 
 namespace rpm {
@@ -594,13 +602,21 @@ static void record_step(rpm_batch* Bh, const BatchDev& B, const Layout& L, cudaS
   a.dot_part = reinterpret_cast<double*>(base + L.dotpart);
   a.dot_count = reinterpret_cast<unsigned*>(base + L.dotcount);
   float2* ya = reinterpret_cast<float2*>(base + L.ya);
+  const int probe_j = m > 1 ? 1 : 0;
+  cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+  check_cuda(cudaStreamIsCapturing(st, &capturing), "capture status");
+  const unsigned probe_flags = capturing == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : 0u;
   for (int j = 0; j < m; ++j) {
     a.in = B.V + (size_t)j * B.ld;
     a.out = B.V + (size_t)(j + 1) * B.ld;
     a.dot_out = &B.st[0].alpha[j];
+    // While capturing, external records become event-record nodes of the graph.
+    if (j == probe_j) check_cuda(cudaEventRecordWithFlags(Bh->probe0, st, probe_flags), "probe record");
     launch_cube<float2>(a, Bh->plan, ya, B.ntraj, st);
+    if (j == probe_j) check_cuda(cudaEventRecordWithFlags(Bh->probe1, st, probe_flags), "probe record");
     k_b_update<<<ew, kEwThreads, 0, st>>>(B, j);
   }
+  Bh->launches_per_step = 1 + 3 * m + 4;
   const size_t ctl_smem = sizeof(double) * 2 * kRecDoubles;
   k_b_control<<<B.ntraj, 128, ctl_smem, st>>>(B);
   k_b_rebuild<<<ew, kEwThreads, 0, st>>>(B);
@@ -694,18 +710,30 @@ static void run_batch(rpm_batch* Bh, int ntraj, const int* sys_of, void* psi, co
     check_cuda(cudaGraphInstantiate(&Bh->exec, Bh->graph, 0), "graph instantiate");
   }
   int active = ntraj;
-  long long replays = 0;
+  long long replays = use_graph ? 1 : 0;  // the eager warm-up step above
+  Bh->kernel_launches += 2 + (use_graph ? Bh->launches_per_step : 0);
   const long long max_replays = cfg.max_steps > 0 ? cfg.max_steps : 10000000LL;
   while (active > 0) {
     for (int r = 0; r < 4; ++r) {
       if (use_graph) check_cuda(cudaGraphLaunch(Bh->exec, st), "graph launch");
       else record_step(Bh, B, L, st);
       ++replays;
+      Bh->kernel_launches += Bh->launches_per_step;
     }
     check_cuda(cudaMemcpyAsync(&active, base + L.active, sizeof(int), cudaMemcpyDeviceToHost, st), "poll");
     check_cuda(cudaStreamSynchronize(st), "poll sync");
+    if (active == ntraj) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, Bh->probe0, Bh->probe1) == cudaSuccess) {
+        Bh->probe_ms_sum += ms;
+        ++Bh->probe_samples;
+      } else {
+        cudaGetLastError();
+      }
+    }
     if (replays > max_replays) fail(RPM_E_NUMERIC, "batched propagation exceeded the step limit");
   }
+  Bh->replays += replays;
   std::vector<TrajState> host(ntraj);
   check_cuda(cudaMemcpyAsync(host.data(), B.st, sizeof(TrajState) * ntraj, cudaMemcpyDeviceToHost, st), "stats");
   check_cuda(cudaStreamSynchronize(st), "stats sync");
@@ -757,6 +785,8 @@ int rpm_batch_create(rpm_system* const* systems, int nsys, const rpm_batch_confi
     check_cuda(cudaStreamCreateWithFlags(&B->work, cudaStreamNonBlocking), "create batch stream");
     check_cuda(cudaEventCreateWithFlags(&B->ev_in, cudaEventDisableTiming), "create event");
     check_cuda(cudaEventCreateWithFlags(&B->ev_out, cudaEventDisableTiming), "create event");
+    check_cuda(cudaEventCreate(&B->probe0), "create probe event");
+    check_cuda(cudaEventCreate(&B->probe1), "create probe event");
     check_cuda(cudaMalloc(&B->views_dev, sizeof(CubeView<float2>) * nsys), "cudaMalloc(views)");
     check_cuda(cudaMemcpy(B->views_dev, views.data(), sizeof(CubeView<float2>) * nsys, cudaMemcpyHostToDevice),
                "copy views");
@@ -782,6 +812,21 @@ int rpm_batch_propagate(rpm_batch* batch, int ntraj, const int* sys_of_host, voi
   });
 }
 
+int rpm_batch_counters(rpm_batch* batch, int reset, long long* kernel_launches, long long* step_replays,
+                       double* hpsi_ms_mean, long long* hpsi_samples) {
+  return guarded([&] {
+    if (!batch) fail(RPM_E_INVALID, "batch is NULL");
+    if (kernel_launches) *kernel_launches = batch->kernel_launches;
+    if (step_replays) *step_replays = batch->replays;
+    if (hpsi_ms_mean) *hpsi_ms_mean = batch->probe_samples ? batch->probe_ms_sum / batch->probe_samples : 0.0;
+    if (hpsi_samples) *hpsi_samples = batch->probe_samples;
+    if (reset) {
+      batch->kernel_launches = batch->replays = batch->probe_samples = 0;
+      batch->probe_ms_sum = 0.0;
+    }
+  });
+}
+
 int rpm_batch_destroy(rpm_batch* batch) {
   return guarded([&] {
     if (!batch) return;
@@ -791,6 +836,8 @@ int rpm_batch_destroy(rpm_batch* batch) {
     if (batch->views_dev) cudaFree(batch->views_dev);
     if (batch->ev_in) cudaEventDestroy(batch->ev_in);
     if (batch->ev_out) cudaEventDestroy(batch->ev_out);
+    if (batch->probe0) cudaEventDestroy(batch->probe0);
+    if (batch->probe1) cudaEventDestroy(batch->probe1);
     if (batch->work) cudaStreamDestroy(batch->work);
     delete batch;
   });
