@@ -85,6 +85,22 @@ int rpm_system_split_tables(const rpm_system* sys, int* lptr, int* lcol, double*
 int rpm_hpsi(rpm_system* sys, int precision, const void* psi_dev, void* out_dev,
              int batch, long long ld, void* stream);
 
+/* rpm_hpsi without any device allocation.  It has no counterpart in the
+ * reference.  It serves callers that may not call cudaMalloc while they run
+ * (run loops of frameworks that own all device memory through a pool or
+ * arena, fixed-budget embedded runtimes, code running while its owner
+ * captures the stream into a CUDA graph).  Its only scratch, batch x ld
+ * elements of the pass-L partial, lives in a 4 MiB array compiled into the
+ * library, which every GPU that loads the library keeps until process exit;
+ * larger batch x ld x element-size requests fail with RPM_E_UNSUPPORTED.
+ * The first call on each device looks up that array's device address (and
+ * sets kernel attributes); make it before any stream capture.  All calls
+ * share the one array: calls that overlap on the GPU (concurrent streams or
+ * threads) race and must be serialised by the caller.  Nothing in the array
+ * needs to start at zero; each call overwrites what it reads. */
+int rpm_hpsi_noalloc(rpm_system* sys, int precision, const void* psi_dev, void* out_dev,
+                     int batch, long long ld, void* stream);
+
 /* FP64 Hermitian Lanczos with two classical Gram-Schmidt passes, replacing
  * ENG:651-688 (AdaptiveLanczosPropagator._basis).  basis_dev holds max_dim
  * complex128 columns of length N (column j at basis_dev + j*N); alpha_dev

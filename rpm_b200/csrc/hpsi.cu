@@ -851,3 +851,97 @@ extern "C" int rpm_hpsi(rpm_system* sys, int precision, const void* psi_dev, voi
     }
   });
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free H psi (rpm_hpsi_noalloc)
+//
+// For callers that must not allocate device memory while they run: host
+// frameworks whose run loop forbids cudaMalloc (their memory comes from a
+// pool or arena they own), embedded runtimes with a fixed memory budget
+// decided at start-up, and code that runs while its owner is capturing a
+// stream into a CUDA graph.  rpm_hpsi grows a per-system cudaMalloc'd buffer
+// for the only scratch the radical-split action needs, the pass-L partial
+// (batch x ld elements).  This variant uses a fixed array compiled into the
+// library instead, so every GPU that loads the library holds those bytes
+// until the process exits.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace rpm {
+
+constexpr size_t kNoAllocScratchBytes = (size_t)4 << 20;  // 4 MiB per GPU
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+static void* g_noalloc_address[kNoAllocMaxDevices];
+static std::mutex g_noalloc_mutex;
+
+// Device address of g_noalloc_scratch on the current device.  In host code
+// the array's name is only a host-side stand-in, so the address is looked up
+// once per device, with that device current, and cached.
+static void* noalloc_scratch() {
+  int dev = 0;
+  check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev < 0 || dev >= kNoAllocMaxDevices) fail(RPM_E_UNSUPPORTED, "rpm_hpsi_noalloc supports device ordinals 0..63");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_address[dev]) {
+    void* p = nullptr;
+    check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(no-alloc scratch)");
+    g_noalloc_address[dev] = p;
+  }
+  return g_noalloc_address[dev];
+}
+
+template <class T>
+static void launch_hpsi_noalloc(rpm_system* sys, const T* in, T* out, int batch, long long ld, cudaStream_t stream) {
+  if (!sys->on_device) fail(RPM_E_INVALID, "system was created host-only");
+  if (batch < 1) return;
+  if (!sys->split) {  // the per-term kernel needs no scratch
+    launch_generic<T>(generic_of<T>(sys), in, out, batch, ld, stream);
+    return;
+  }
+  const size_t need = (size_t)batch * (size_t)ld * sizeof(T);
+  if (need > kNoAllocScratchBytes) {
+    fail(RPM_E_UNSUPPORTED, "rpm_hpsi_noalloc: batch x ld x element size = " + std::to_string(need) +
+                                " bytes exceeds its fixed 4 MiB scratch; use rpm_hpsi or a smaller batch");
+  }
+  T* ya = static_cast<T*>(noalloc_scratch());
+  if (sys->cube && sys->cube64.inner_l >= 1 && sys->cube64.inner_r >= 1) {
+    HpsiArgs<T> a{};
+    a.in = in;
+    a.out = out;
+    a.ld = ld;
+    a.views = cube_dev_of<T>(sys);
+    rpm_system* one[1] = {sys};
+    launch_cube<T>(a, cube_plan(one, 1), ya, batch, stream);
+    return;
+  }
+  const SplitView<T>& s = split_of<T>(sys);
+  const bool a_ok = try_pass_a<T, 4>(s, in, ya, batch, ld, stream) || try_pass_a<T, 2>(s, in, ya, batch, ld, stream);
+  if (a_ok && (try_pass_b<T, 4, 8>(s, in, ya, out, batch, ld, stream) ||
+               try_pass_b<T, 2, 4>(s, in, ya, out, batch, ld, stream)))
+    return;
+  fail(RPM_E_UNSUPPORTED, "rpm_hpsi_noalloc: radical groups too large for the shared-memory kernels");
+}
+
+}  // namespace rpm
+
+extern "C" int rpm_hpsi_noalloc(rpm_system* sys, int precision, const void* psi_dev, void* out_dev, int batch,
+                                long long ld, void* stream) {
+  return rpm::guarded([&] {
+    if (!sys) rpm::fail(RPM_E_INVALID, "system is NULL");
+    if (!psi_dev || !out_dev) rpm::fail(RPM_E_INVALID, "NULL state pointer");
+    if (batch < 0 || (batch > 0 && ld < sys->n)) rpm::fail(RPM_E_INVALID, "invalid batch or leading dimension");
+    if (psi_dev == out_dev) rpm::fail(RPM_E_INVALID, "H psi cannot run in place");
+    auto st = static_cast<cudaStream_t>(stream);
+    if (precision == RPM_PREC_C128) {
+      rpm::launch_hpsi_noalloc<double2>(sys, static_cast<const double2*>(psi_dev), static_cast<double2*>(out_dev),
+                                        batch, ld, st);
+    } else if (precision == RPM_PREC_C64) {
+      rpm::launch_hpsi_noalloc<float2>(sys, static_cast<const float2*>(psi_dev), static_cast<float2*>(out_dev), batch,
+                                       ld, st);
+    } else {
+      rpm::fail(RPM_E_INVALID, "precision must be 64 or 128");
+    }
+  });
+}
