@@ -85,6 +85,13 @@ int rpm_system_split_tables(const rpm_system* sys, int* lptr, int* lcol, double*
 int rpm_hpsi(rpm_system* sys, int precision, const void* psi_dev, void* out_dev,
              int batch, long long ld, void* stream);
 
+/* Select the cube-kernel variant used by every later H psi launch (process
+ * wide; 0 = built-in heuristic): inner spin-1/2 digits per radical cube
+ * (ni_l, ni_r in {1, 2}), pass-L column tile tr in {1, 2, 4, 8} and pass-R
+ * row tile tl in {1, ..., 16}.  A choice that cannot run for a system falls
+ * back to the heuristic.  Used by the autotuner; no reference counterpart. */
+int rpm_set_cube_tuning(int ni_l, int ni_r, int tr, int tl);
+
 /* rpm_hpsi without any device allocation.  It has no counterpart in the
  * reference.  It serves callers that may not call cudaMalloc while they run
  * (run loops of frameworks that own all device memory through a pool or

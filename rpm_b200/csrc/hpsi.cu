@@ -635,6 +635,12 @@ int sm_count() {
 
 static constexpr size_t kMaxSmem = 200 * 1024;
 
+// Explicit cube-kernel variant (0 = heuristic), set by rpm_set_cube_tuning.
+struct CubeTuning {
+  int ni_l, ni_r, tr, tl;
+};
+static CubeTuning g_cube_tuning{0, 0, 0, 0};
+
 // Raise a kernel's dynamic shared-memory limit only when needed, so that
 // launches recorded into a CUDA graph issue no attribute calls once warmed up.
 template <class K>
@@ -682,6 +688,13 @@ static bool try_cube_r(const HpsiArgs<T>& a, const CubePlan& p, const T* ya, int
 // enough that small batches still produce about two CTAs per SM.
 template <class T, int NI>
 static void cube_l_dispatch(const HpsiArgs<T>& a, const CubePlan& p, T* ya, int batch, cudaStream_t st) {
+  switch (g_cube_tuning.tr) {  // explicit choice (autotuner); falls back to the heuristic if it cannot run
+    case 8: if (try_cube_l<T, NI, 8>(a, p, ya, batch, st)) return; break;
+    case 4: if (try_cube_l<T, NI, 4>(a, p, ya, batch, st)) return; break;
+    case 2: if (try_cube_l<T, NI, 2>(a, p, ya, batch, st)) return; break;
+    case 1: if (try_cube_l<T, NI, 1>(a, p, ya, batch, st)) return; break;
+    default: break;
+  }
   const int want = 2 * sm_count();
   auto tiles = [&](int tr) { return ((p.half_r + tr - 1) / tr) * batch; };
   if (tiles(8) >= want && try_cube_l<T, NI, 8>(a, p, ya, batch, st)) return;
@@ -693,6 +706,14 @@ static void cube_l_dispatch(const HpsiArgs<T>& a, const CubePlan& p, T* ya, int 
 
 template <class T, int NI>
 static void cube_r_dispatch(const HpsiArgs<T>& a, const CubePlan& p, const T* ya, int batch, cudaStream_t st) {
+  switch (g_cube_tuning.tl) {
+    case 16: if (try_cube_r<T, NI, 16>(a, p, ya, batch, st)) return; break;
+    case 8: if (try_cube_r<T, NI, 8>(a, p, ya, batch, st)) return; break;
+    case 4: if (try_cube_r<T, NI, 4>(a, p, ya, batch, st)) return; break;
+    case 2: if (try_cube_r<T, NI, 2>(a, p, ya, batch, st)) return; break;
+    case 1: if (try_cube_r<T, NI, 1>(a, p, ya, batch, st)) return; break;
+    default: break;
+  }
   const int want = 2 * sm_count();
   auto ctas = [&](int tl) { return ((p.nl + tl - 1) / tl) * batch; };
   if (ctas(16) >= want && try_cube_r<T, NI, 16>(a, p, ya, batch, st)) return;
@@ -705,7 +726,9 @@ static void cube_r_dispatch(const HpsiArgs<T>& a, const CubePlan& p, const T* ya
 
 template <class T>
 void launch_cube(const HpsiArgs<T>& a, const CubePlan& p, T* ya, int batch, cudaStream_t st) {
-  if (p.ni_l >= 2) {
+  const int ni_l = g_cube_tuning.ni_l > 0 ? std::min(g_cube_tuning.ni_l, p.ni_l) : p.ni_l;
+  const int ni_r = g_cube_tuning.ni_r > 0 ? std::min(g_cube_tuning.ni_r, p.ni_r) : p.ni_r;
+  if (ni_l >= 2) {
     HpsiArgs<T> al = a;
     al.dot_part = nullptr;
     cube_l_dispatch<T, 2>(al, p, ya, batch, st);
@@ -714,7 +737,7 @@ void launch_cube(const HpsiArgs<T>& a, const CubePlan& p, T* ya, int batch, cuda
     al.dot_part = nullptr;
     cube_l_dispatch<T, 1>(al, p, ya, batch, st);
   }
-  if (p.ni_r >= 2) {
+  if (ni_r >= 2) {
     cube_r_dispatch<T, 2>(a, p, ya, batch, st);
   } else {
     cube_r_dispatch<T, 1>(a, p, ya, batch, st);
@@ -833,6 +856,19 @@ template void launch_cube<double2>(const HpsiArgs<double2>&, const CubePlan&, do
 template void launch_cube<float2>(const HpsiArgs<float2>&, const CubePlan&, float2*, int, cudaStream_t);
 
 }  // namespace rpm
+
+extern "C" int rpm_set_cube_tuning(int ni_l, int ni_r, int tr, int tl) {
+  return rpm::guarded([&] {
+    auto ok = [](int v, std::initializer_list<int> allowed) {
+      for (int a : allowed)
+        if (v == a) return true;
+      return false;
+    };
+    if (!ok(ni_l, {0, 1, 2}) || !ok(ni_r, {0, 1, 2}) || !ok(tr, {0, 1, 2, 4, 8}) || !ok(tl, {0, 1, 2, 4, 8, 16}))
+      rpm::fail(RPM_E_INVALID, "cube tuning: ni in {0,1,2}, tr in {0,1,2,4,8}, tl in {0,1,2,4,8,16}");
+    rpm::g_cube_tuning = rpm::CubeTuning{ni_l, ni_r, tr, tl};
+  });
+}
 
 extern "C" int rpm_hpsi(rpm_system* sys, int precision, const void* psi_dev, void* out_dev, int batch, long long ld,
                         void* stream) {
