@@ -220,6 +220,7 @@ def b200_arm(args, rank: int, world: int, dist) -> None:
     import rpm_b200 as rb
     from rpm_b200 import synthetic
     from rpm_b200.batched import BatchedPropagator
+    from rpm_b200.distributed import gather_yields, max_over_ranks
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     torch.cuda.set_device(dev)
@@ -269,20 +270,11 @@ def b200_arm(args, rank: int, world: int, dist) -> None:
     if dist is not None:
         dist.barrier()
     clock_info = clocks.stop()
-    elapsed = t_start.elapsed_time(t_end) / 1e3
-    if dist is not None:
-        t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+    elapsed = max_over_ranks(t_start.elapsed_time(t_end) / 1e3, dist, dev)
     counters = bp.counters(reset=True)
     value = args.steps * ntraj * world / elapsed
     yields = bp.yields_device(times, values, LIFETIME_US)
-    if dist is not None:
-        gathered = torch.empty(world * ntraj, dtype=torch.float64, device=dev)
-        dist.all_gather_into_tensor(gathered, yields)
-        yields_all = gathered
-    else:
-        yields_all = yields
+    yields_all = gather_yields(yields, dist)  # the only cross-rank data: per-trajectory yields
     bad = [s.status for s in stats if s.status]
     if bad:
         raise RuntimeError(f"batched propagation failed with status {bad[0]}")
@@ -299,11 +291,7 @@ def b200_arm(args, rank: int, world: int, dist) -> None:
         res = bp.propagate(host_states, times, system_index=system_index, lifetime_us=LIFETIME_US)
     e1.record()
     torch.cuda.synchronize()
-    e2e_elapsed = e0.elapsed_time(e1) / 1e3
-    if dist is not None:
-        t = torch.tensor([e2e_elapsed], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_elapsed = float(t.item())
+    e2e_elapsed = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist, dev)
     e2e_value = e2e_steps * ntraj * world / e2e_elapsed
     h2d = ntraj * n * 16
     d2h = res.observable_values.nbytes + res.state_error_estimates.nbytes + res.yields.nbytes
