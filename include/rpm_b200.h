@@ -166,6 +166,14 @@ int rpm_norm(rpm_system* sys, const void* psi_dev, double* norm_host, void* stre
 int rpm_simpson_yield(const double* times_dev, const double* pops_dev, int n, int batch,
                       long long ld, double lifetime_us, double* yields_dev, void* stream);
 
+/* out = (1 (x) .. (x) U (x) .. (x) 1) in for a d x d complex128 operator U
+ * (row-major, host) acting on tensor axis `axis`, for `batch` complex128
+ * vectors spaced `ld` apart.  Replaces poster_reproduction/core.py:285-292
+ * (local_unitary_apply), the instantaneous nuclear pulse between segments of
+ * rpm_nuclear_spin_rotation_control.py:281-308. */
+int rpm_apply_local_operator(const int* dims, int ndims, int axis, const double* op_host,
+                             const void* in_dev, void* out_dev, int batch, long long ld, void* stream);
+
 /* ---------------------------------------------------------------------------
  * Batched mixed-precision propagation: many trajectories (state vectors of
  * one or more systems, e.g. field orientations or bath sizes) advanced

@@ -708,3 +708,53 @@ def coarse_grid_indices(n_points: int, stride: int = 2) -> np.ndarray:
     if idx[-1] != n_points - 1:
         idx = np.append(idx, n_points - 1)
     return idx
+
+
+# ---------------------------------------------------------------------------
+# Segment propagation (rpm_nuclear_spin_rotation_control.py:281-308)
+# ---------------------------------------------------------------------------
+
+def local_unitary_apply(state, dimensions, axis, unitary) -> np.ndarray:
+    """d x d operator on one tensor axis (poster_reproduction/core.py:285-292)."""
+    t = np.asarray(state, dtype=complex).reshape(tuple(dimensions))
+    front = np.moveaxis(t, int(axis), 0)
+    out = (np.asarray(unitary, dtype=complex) @ front.reshape(dimensions[axis], -1)).reshape(front.shape)
+    return np.moveaxis(out, 0, axis).reshape(-1)
+
+
+def propagate_segments(initial_state, times_us, segments, *, state_error_budget=2.4e-5, **knobs):
+    """The reference's pulsed loop; ``segments`` are (end_us, hamiltonian, pulse|None).
+
+    Returns (values, bounds, final_state, (accepted, rejected, matvecs), accumulated_error).
+    """
+    times = np.asarray(times_us, dtype=float)
+    dims = segments[0][1].dimensions
+    obs = SingletPopulationObservable(dims)
+    state = np.asarray(initial_state, dtype=complex).reshape(-1)
+    values, bounds = np.empty(times.size), np.empty(times.size)
+    values[0], bounds[0] = singlet_population(state, dims), 0.0
+    cursor, current, acc = 1, 0.0, 0.0
+    counts = [0, 0, 0]
+    for end, ham, pulse in segments:
+        boundary = float(end)
+        stop = int(np.searchsorted(times, boundary + 1e-12, side="right"))
+        requested = times[cursor:stop] - current
+        duration = boundary - current
+        local = requested if requested.size and requested[-1] >= duration - 1e-12 else np.append(requested, duration)
+        if duration > 0.0:
+            prop = AdaptiveLanczosPropagator(ham, **knobs)
+            prop.state_error_budget = state_error_budget * duration / times[-1]
+            res = prop.propagate(state, local, obs)
+            k = requested.size
+            values[cursor:stop] = res.observable_values[:k]
+            glob = acc + res.state_error_estimates[:k]
+            bounds[cursor:stop] = 2.0 * glob + glob ** 2
+            state = res.final_state
+            counts[0] += res.stats.accepted_steps
+            counts[1] += res.stats.rejected_steps
+            counts[2] += res.stats.matvecs
+            acc += res.stats.accumulated_state_error
+        cursor, current = stop, boundary
+        if pulse is not None and boundary < times[-1] - 1e-12:
+            state = local_unitary_apply(state, dims, pulse[0], pulse[1])
+    return values, bounds, state, tuple(counts), acc

@@ -697,3 +697,52 @@ int rpm_simpson_yield(const double* times_dev, const double* pops_dev, int n, in
 }
 
 }  // extern "C"
+
+namespace rpm {
+
+// out = (1 (x) ... (x) U (x) ... (x) 1) in for a d x d operator U on one axis
+// (any operator; used for instantaneous unitaries between propagation segments).
+__global__ void __launch_bounds__(256) k_apply_local(const double2* __restrict__ in, double2* __restrict__ out,
+                                                    long long n, long long ld, long long stride, int d,
+                                                    const double2* __restrict__ op) {
+  const double2* u = op;  // d x d, read through the read-only cache
+  const double2* x = in + (long long)blockIdx.y * ld;
+  double2* y = out + (long long)blockIdx.y * ld;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int digit = (int)((i / stride) % d);
+    const long long base = i - (long long)digit * stride;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int c = 0; c < d; ++c) acc = cfma(__ldg(u + digit * d + c), x[base + (long long)c * stride], acc);
+    y[i] = acc;
+  }
+}
+
+}  // namespace rpm
+
+extern "C" int rpm_apply_local_operator(const int* dims, int ndims, int axis, const double* op_host, const void* in_dev,
+                                        void* out_dev, int batch, long long ld, void* stream) {
+  return guarded([&] {
+    if (!dims || ndims < 1 || ndims > RPM_MAX_AXES || !op_host || !in_dev || !out_dev || batch < 1)
+      fail(RPM_E_INVALID, "bad arguments");
+    if (axis < 0 || axis >= ndims) fail(RPM_E_INVALID, "axis out of range");
+    if (in_dev == out_dev) fail(RPM_E_INVALID, "local operator cannot be applied in place");
+    long long n = 1, stride = 1;
+    for (int a = 0; a < ndims; ++a) {
+      if (dims[a] < 1) fail(RPM_E_INVALID, "Every tensor dimension must be positive.");
+      n *= dims[a];
+    }
+    for (int a = ndims - 1; a > axis; --a) stride *= dims[a];
+    if (ld < n) fail(RPM_E_INVALID, "leading dimension smaller than the state");
+    const int d = dims[axis];
+    if (d > RPM_MAX_LOCAL_DIM) fail(RPM_E_UNSUPPORTED, "axis dimension above 64");
+    auto st = static_cast<cudaStream_t>(stream);
+    double2* d_op = nullptr;
+    check_cuda(cudaMallocAsync(&d_op, sizeof(double2) * d * d, st), "cudaMallocAsync(op)");
+    check_cuda(cudaMemcpyAsync(d_op, op_host, sizeof(double2) * d * d, cudaMemcpyHostToDevice, st), "copy op");
+    const int blocks = (int)std::min<long long>((n + 255) / 256, 4096);
+    k_apply_local<<<dim3(blocks, batch), 256, 0, st>>>(static_cast<const double2*>(in_dev),
+                                                       static_cast<double2*>(out_dev), n, ld, stride, d, d_op);
+    check_launch("k_apply_local");
+    check_cuda(cudaFreeAsync(d_op, st), "cudaFreeAsync(op)");
+  });
+}
