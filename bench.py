@@ -213,6 +213,46 @@ def reference_arm(args, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def hpsi_probe(args) -> None:
+    """Complex64 H psi alone: ``--hpsi-only K`` times K launches over
+    orientations x vectors full-size states of one orientation (the batched
+    step's H psi shape) and prints one diagnostic JSON line.  Used for kernel
+    timing and as a short ncu target; not a benchmark line."""
+    import torch
+
+    import rpm_b200 as rb
+    from rpm_b200 import _lib, synthetic
+
+    full = synthetic.full_system()
+    h = rb.CompiledFullPairHamiltonian(full.dimensions, full.terms(math.pi / 4, 0.0), left_axes=full.left_axes,
+                                       right_axes=full.right_axes)
+    n = full.dimension
+    batch = args.orientations * args.vectors
+    ld = (n + 63) // 64 * 64
+    g = torch.Generator(device="cuda").manual_seed(5)
+    x = torch.randn((batch, ld), dtype=torch.complex64, device="cuda", generator=g)
+    y = torch.empty_like(x)
+
+    def launch():
+        _lib.call("rpm_hpsi", h._system.handle, _lib.PREC_C64, _lib.ptr(x), _lib.ptr(y), batch, ld,
+                  _lib.stream_handle())
+
+    for _ in range(max(3, args.warmup)):
+        launch()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.hpsi_only):
+        launch()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.hpsi_only
+    peak, _ = measured_peak_hbm()
+    gbs = 16.0 * n * batch / (ms * 1e-3) / 1e9
+    print(json.dumps({"probe": "hpsi_c64", "vectors": batch, "n": n, "fast_kernels": h._system.fast_hpsi,
+                      "ms_per_launch_pair": ms, "algorithmic_GBps": gbs, "hbm_frac": gbs / peak}), flush=True)
+
+
 def b200_arm(args, rank: int, world: int, dist) -> None:
     import numpy as np
     import torch
@@ -372,9 +412,14 @@ def main() -> None:
     p.add_argument("--cpu-horizon", type=float, default=0.025, help="us of the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison trajectory")
+    p.add_argument("--hpsi-only", type=int, default=0, metavar="K",
+                   help="diagnostic: time K complex64 H psi launches over orientations x vectors states and exit")
     args = p.parse_args()
     if args.warmup < 0 or args.steps < 1:
         raise SystemExit("steps must be >= 1 and warmup >= 0")
+    if args.hpsi_only > 0:
+        hpsi_probe(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = None

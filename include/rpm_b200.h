@@ -92,6 +92,12 @@ int rpm_hpsi(rpm_system* sys, int precision, const void* psi_dev, void* out_dev,
  * back to the heuristic.  Used by the autotuner; no reference counterpart. */
 int rpm_set_cube_tuning(int ni_l, int ni_r, int tr, int tl);
 
+/* *usable = 1 when complex64 H psi of this system runs on the shape-
+ * specialised kernels (axes ordered electron A, electron B, left nuclei,
+ * right nuclei; each radical's spin-1 nuclei before its spin-1/2 nuclei;
+ * a compiled digit pattern), else 0.  Diagnostic; no reference counterpart. */
+int rpm_system_fast_hpsi(const rpm_system* sys, int* usable);
+
 /* rpm_hpsi without any device allocation.  It has no counterpart in the
  * reference.  It serves callers that may not call cudaMalloc while they run
  * (run loops of frameworks that own all device memory through a pool or

@@ -23,6 +23,7 @@
 //
 // * Generic per-term mode product for systems without a radical split.
 #include <algorithm>
+#include <type_traits>
 
 #include "common.cuh"
 #include "hpsi.cuh"
@@ -726,6 +727,10 @@ static void cube_r_dispatch(const HpsiArgs<T>& a, const CubePlan& p, const T* ya
 
 template <class T>
 void launch_cube(const HpsiArgs<T>& a, const CubePlan& p, T* ya, int batch, cudaStream_t st) {
+  if constexpr (std::is_same<T, float2>::value) {
+    const bool tuned = g_cube_tuning.ni_l || g_cube_tuning.ni_r || g_cube_tuning.tr || g_cube_tuning.tl;
+    if (!tuned && launch_cube_fast(a, p, ya, batch, st)) return;
+  }
   const int ni_l = g_cube_tuning.ni_l > 0 ? std::min(g_cube_tuning.ni_l, p.ni_l) : p.ni_l;
   const int ni_r = g_cube_tuning.ni_r > 0 ? std::min(g_cube_tuning.ni_r, p.ni_r) : p.ni_r;
   if (ni_l >= 2) {
@@ -817,6 +822,7 @@ CubePlan cube_plan(rpm_system* const* systems, int nsys) {
     p.n_outer_l2 = std::max(p.n_outer_l2, outer(s->cube_l, 2));
     p.n_outer_r1 = std::max(p.n_outer_r1, outer(s->cube_r, 1));
     p.n_outer_r2 = std::max(p.n_outer_r2, outer(s->cube_r, 2));
+    fast_plan_add(p, s, k == 0);
   }
   p.tab_cap = (p.tab_cap + 1) & ~1;
   if (p.ni_l < 1 || p.ni_r < 1) fail(RPM_E_UNSUPPORTED, "cube kernels need a trailing spin-1/2 digit per radical");

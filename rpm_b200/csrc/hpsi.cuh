@@ -31,10 +31,19 @@ struct CubePlan {
   int nl, nr, half_r, tab_cap;
   int ni_l, ni_r;  // inner digits used per side
   int n_outer_l1, n_outer_l2, n_outer_r1, n_outer_r2;  // outer-index counts for NI = 1, 2
+  // shape-specialised complex64 passes (hpsi_fast.cu): usable when every
+  // system of the launch has the standard axis order and the same digit
+  // pattern (spin-1 count, spin-1/2 count) per radical
+  int fast;
+  int fl_n1, fl_nh, fr_n1, fr_nh, f_half_l, f_half_r;
 };
 
 int sm_count();
 CubePlan cube_plan(rpm_system* const* systems, int nsys);
+void fast_plan_add(CubePlan& p, const rpm_system* s, bool first);
+// Launches the specialised passes; false (nothing launched) when the plan or
+// the pointers/strides (16-byte alignment) do not allow them.
+bool launch_cube_fast(const HpsiArgs<float2>& a, const CubePlan& p, float2* ya, int batch, cudaStream_t stream);
 // Two passes: pass L into `ya` (batch x ld scratch), pass R into a.out.
 template <class T>
 void launch_cube(const HpsiArgs<T>& a, const CubePlan& p, T* ya, int batch, cudaStream_t stream);

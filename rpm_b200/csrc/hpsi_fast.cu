@@ -1,0 +1,590 @@
+// Shape-specialised complex64 H psi passes for the standard radical layout.
+//
+// Scope: radical-split systems whose tensor axes are ordered
+// (electron A, electron B, left nuclei..., right nuclei...) -- the order of
+// the reference's production system (rpm_statevector_engine.py:367-469,
+// poster_reproduction/core.py:172-229) -- so that the state is the C-order
+// array psi[eA][eB][l][r] with l over the left nuclei (HL values) and r over
+// the right nuclei (HR values), and whose radicals each list their spin-1
+// nuclei before their spin-1/2 nuclei.  The nuclear digit pattern of both
+// radicals is a template parameter, so every digit stride, table offset and
+// loop bound below is a compile-time constant.
+//
+// The action is the one of the cube form in hpsi.cu (same tables, same
+// merged diagonal / electron-flip coefficients, same pair operator), with
+// the two passes in the opposite order:
+//   pass R: yb = sf (1 (x) R) psi            pass L: out = sf (L (x) 1 + P) psi + yb
+// but the thread mapping is chosen so that every coefficient a warp needs at
+// a time is the same for all 32 lanes:
+//   * pass R: a CTA stages 32 rows (eA, l) x all (eB, r) of one vector; lane
+//     = row.  R's coefficients depend on (eB, r) only, which is uniform in a
+//     warp task, so they are shared-memory broadcasts.  Each thread holds a
+//     register cube (eB x the two fastest spin-1/2 digits) of its row.
+//   * pass L: a CTA stages every l of 16 columns (eB x 8 consecutive r);
+//     lane = column (+ one spin-1/2 digit of l as lane bit 4).  L's
+//     coefficients depend on l only; the lane-bit digit and eB (for the pair
+//     operator) are fixed per lane for the whole kernel.
+// Partners along register digits come from registers, all others from the
+// staged tile (conflict-free: padded rows in pass R, 128-byte rows in pass L).
+// Pass R stores its partial row-wise (each lane 32 contiguous bytes); pass L
+// reads it column-coalesced, prefetched at the start of each task, and fuses
+// <psi, H psi>.  Pass L walks the batch in reverse order so that the partials
+// and inputs written or read last are still in L2 when it starts.
+#include <utility>
+#include <vector>
+
+#include "common.cuh"
+#include "hpsi.cuh"
+
+namespace rpm {
+namespace {
+
+constexpr int ipow3(int n) { return n == 0 ? 1 : 3 * ipow3(n - 1); }
+
+// Digit k of a radical's nuclei (k = 0 slowest): spin-1 for k < N1, spin-1/2
+// after.  Table offsets follow build_cube_side: [Zd0, Zd1, Zf0, Zf1], then per
+// nucleus D (2d), F (2d), X ((2d)^2).
+template <int N1, int NH>
+struct Shape {
+  static constexpr int K = N1 + NH;
+  static constexpr int HALF = ipow3(N1) << NH;
+  static constexpr int dim(int k) { return k < N1 ? 3 : 2; }
+  static constexpr int gs(int k) {
+    int s = 1;
+    for (int q = K - 1; q > k; --q) s *= dim(q);
+    return s;
+  }
+  static constexpr int offD(int k) {
+    int o = 4;
+    for (int q = 0; q < k; ++q) o += 4 * dim(q) + 4 * dim(q) * dim(q);
+    return o;
+  }
+  static constexpr int offF(int k) { return offD(k) + 2 * dim(k); }
+  static constexpr int offX(int k) { return offD(k) + 4 * dim(k); }
+  static constexpr int NTAB = offD(K);
+};
+
+// Per outer index: diagonal and electron-flip coefficients merged over the
+// electron-only term and every outer digit.
+struct ORec {
+  float d[2];
+  float2 f[2];
+};
+
+constexpr int align16c(int bytes) { return (bytes + 15) & ~15; }
+
+__device__ __forceinline__ void copy16(void* smem_dst, const void* gmem_src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void copy_wait_all() { asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory"); }
+
+__device__ __forceinline__ float2 rmacf(float d, float2 x, float2 acc) {
+  acc.x = fmaf(d, x.x, acc.x);
+  acc.y = fmaf(d, x.y, acc.y);
+  return acc;
+}
+
+__device__ __forceinline__ bool skip_vec(const HpsiArgs<float2>& a, int b) {
+  return a.skip && a.skip[(long long)b * a.skip_stride] != 0;
+}
+__device__ __forceinline__ double in_scale(const HpsiArgs<float2>& a, int b) {
+  return a.in_scale ? a.in_scale[(long long)b * a.scale_stride] : 1.0;
+}
+
+// Fused <in_scaled, H in_scaled>: per-block partial; the last block of
+// vector b sums the partials in block order (deterministic).
+__device__ void finish_dot_fast(const HpsiArgs<float2>& a, int b, double mine) {
+  __shared__ double red[32];
+  __shared__ bool last;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mine;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
+    a.dot_part[(long long)b * gridDim.x + blockIdx.x] = tot;
+    __threadfence();
+    last = atomicAdd(a.dot_count + b, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    double s = 0.0;
+    for (int k = 0; k < (int)gridDim.x; ++k) s += __ldcg(a.dot_part + (long long)b * gridDim.x + k);
+    a.dot_out[(long long)b * a.dot_stride] = s;
+    a.dot_count[b] = 0;
+  }
+}
+
+// Merged diagonal / flip coefficients of the two register-cube digits
+// (digits K-2 -> bit 1 of i, K-1 -> bit 0 of i).
+template <class S>
+__device__ __forceinline__ void cube_consts(const float2* tab, float (&din)[2][4], float2 (&fin)[2][4]) {
+  constexpr int K = S::K;
+#pragma unroll
+  for (int e = 0; e < 2; ++e)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      din[e][i] = tab[S::offD(K - 2) + e * 2 + (i >> 1)].x + tab[S::offD(K - 1) + e * 2 + (i & 1)].x;
+      fin[e][i] = cadd(tab[S::offF(K - 2) + e * 2 + (i >> 1)], tab[S::offF(K - 1) + e * 2 + (i & 1)]);
+    }
+}
+
+// Register-cube transitions of the two cube digits.
+template <class S>
+__device__ __forceinline__ void cube_inner(const float2* tab, const float2 (&x)[2][4], float2 (&acc)[2][4]) {
+  constexpr int K = S::K;
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const float2* X = tab + S::offX(K - 2 + q);
+    const int sh = 1 - q;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int bit = (i >> sh) & 1;
+      const int ip = i ^ (1 << sh);
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        acc[e][i] = cfma(X[(e * 2 + bit) * 4 + (1 - bit)], x[0][ip], acc[e][i]);
+        acc[e][i] = cfma(X[(e * 2 + bit) * 4 + 2 + (1 - bit)], x[1][ip], acc[e][i]);
+      }
+    }
+  }
+}
+
+// acc[e][i] += c[e][ep] * y[ep][i]
+__device__ __forceinline__ void partner_mac(const float2 (&c)[2][2], const float2 (&y)[2][4], float2 (&acc)[2][4]) {
+#pragma unroll
+  for (int ep = 0; ep < 2; ++ep)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      acc[0][i] = cfma(c[0][ep], y[ep][i], acc[0][i]);
+      acc[1][i] = cfma(c[1][ep], y[ep][i], acc[1][i]);
+    }
+}
+
+// Coefficients of one partner along outer digit k (value m -> mp) for every
+// (output electron e, input electron ep).
+template <class S>
+__device__ __forceinline__ void outer_coefs(const float2* tab, int k, int m, int mp, float2 (&c)[2][2]) {
+  const float2* X = tab + S::offX(k);
+  const int d = S::dim(k);
+#pragma unroll
+  for (int e = 0; e < 2; ++e)
+#pragma unroll
+    for (int ep = 0; ep < 2; ++ep) c[e][ep] = X[(e * d + m) * 2 * d + ep * d + mp];
+}
+
+// ---------------------------------------------------------------------------
+// Pass R: 32 rows (eA, l) x all (eB, r) per CTA; lane = row.
+// ---------------------------------------------------------------------------
+template <int N1, int NH>
+struct PassR {
+  using S = Shape<N1, NH>;
+  static constexpr int HR = S::HALF;
+  static constexpr int NO = HR / 4;      // outer indices per row
+  static constexpr int RS = 2 * HR + 2;  // padded row stride (elements): an odd number of 16-byte units
+  static constexpr int TAB_BYTES = align16c(S::NTAB * 8);
+  static constexpr int OREC_BYTES = align16c(NO * (int)sizeof(ORec));
+  static constexpr int SMEM = TAB_BYTES + OREC_BYTES + 32 * RS * 8;
+  // 8 warps: measured faster than 12 or 16, which force register spills
+  static constexpr int WARPS = NO % 8 == 0 ? 8 : NO % 6 == 0 ? 6 : NO % 4 == 0 ? 4 : NO % 3 == 0 ? 3 : NO < 8 ? NO : 8;
+  static_assert(NH >= 2, "pass R needs two trailing spin-1/2 digits");
+};
+
+template <int N1, int NH>
+__global__ void __launch_bounds__(PassR<N1, NH>::WARPS * 32, 2)
+    fast_pass_r(HpsiArgs<float2> a, float2* __restrict__ yb) {
+  using P = PassR<N1, NH>;
+  using S = typename P::S;
+  constexpr int K = S::K;
+  constexpr int HR = P::HR, NO = P::NO, RS = P::RS;
+  constexpr int NT = P::WARPS * 32;
+  const int b = blockIdx.y;
+  if (skip_vec(a, b)) return;
+  const CubeView<float2>* view = a.views + (a.sys_of ? a.sys_of[b] : 0);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* tab = reinterpret_cast<float2*>(smem_raw);
+  ORec* orec = reinterpret_cast<ORec*>(smem_raw + P::TAB_BYTES);
+  float2* tile = reinterpret_cast<float2*>(smem_raw + P::TAB_BYTES + P::OREC_BYTES);
+  const int half_l = view->half_l;
+  const int row0 = blockIdx.x * 32;
+  const int rows = min(32, 2 * half_l - row0);
+  const long long quarter = (long long)half_l * HR;
+  const float2* x_in = a.in + (long long)b * a.ld;
+  constexpr int CH = HR / 2;  // 16-byte chunks per half row
+  for (int idx = threadIdx.x; idx < rows * 2 * CH; idx += NT) {
+    const int rr = idx / (2 * CH), rem = idx - rr * (2 * CH);
+    const int e = rem / CH, c = rem - e * CH;
+    const int rho = row0 + rr;
+    const int ea = rho >= half_l ? 1 : 0;
+    const int llo = rho - ea * half_l;
+    copy16(tile + rr * RS + e * HR + 2 * c, x_in + (2 * ea + e) * quarter + (long long)llo * HR + 2 * c);
+  }
+  for (int k = threadIdx.x; k < S::NTAB; k += NT) tab[k] = view->tabR[k];
+  __syncthreads();
+  for (int o = threadIdx.x; o < NO; o += NT) {
+    ORec r;
+    r.d[0] = tab[0].x;
+    r.d[1] = tab[1].x;
+    r.f[0] = tab[2];
+    r.f[1] = tab[3];
+#pragma unroll
+    for (int k = 0; k < K - 2; ++k) {
+      const int m = (o / (S::gs(k) / 4)) % S::dim(k);
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        r.d[e] += tab[S::offD(k) + e * S::dim(k) + m].x;
+        r.f[e] = cadd(r.f[e], tab[S::offF(k) + e * S::dim(k) + m]);
+      }
+    }
+    orec[o] = r;
+  }
+  copy_wait_all();
+  __syncthreads();
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const float sf = (float)in_scale(a, b);
+  const float2* rowp = tile + lane * RS;
+  float din[2][4];
+  float2 fin[2][4];
+  cube_consts<S>(tab, din, fin);
+  const int rho = row0 + lane;
+  const int ea = rho >= half_l ? 1 : 0;
+  const long long gbase = 2 * ea * quarter + (long long)(rho - ea * half_l) * HR;
+  float2* y_b = yb + (long long)b * (a.ya_ld ? a.ya_ld : a.ld) + gbase;
+  for (int o = warp; o < NO; o += P::WARPS) {
+    const ORec rec = orec[o];
+    auto load = [&](int delta, float2 (&y)[2][4]) {
+#pragma unroll
+      for (int ep = 0; ep < 2; ++ep) {
+        const float4 u = *reinterpret_cast<const float4*>(rowp + ep * HR + 4 * o + delta);
+        const float4 v = *reinterpret_cast<const float4*>(rowp + ep * HR + 4 * o + delta + 2);
+        y[ep][0] = make_float2(u.x, u.y);
+        y[ep][1] = make_float2(u.z, u.w);
+        y[ep][2] = make_float2(v.x, v.y);
+        y[ep][3] = make_float2(v.z, v.w);
+      }
+    };
+    float2 x[2][4], acc[2][4];
+    load(0, x);
+#pragma unroll
+    for (int e = 0; e < 2; ++e)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        acc[e][i] = rmacf(rec.d[e] + din[e][i], x[e][i], make_float2(0.f, 0.f));
+        acc[e][i] = cfma(cadd(rec.f[e], fin[e][i]), x[1 - e][i], acc[e][i]);
+      }
+    cube_inner<S>(tab, x, acc);
+#pragma unroll
+    for (int k = 0; k < K - 2; ++k) {
+      const int m = (o / (S::gs(k) / 4)) % S::dim(k);
+#pragma unroll
+      for (int t = 1; t < S::dim(k); ++t) {
+        const int mp = m + t >= S::dim(k) ? m + t - S::dim(k) : m + t;
+        float2 c[2][2], y[2][4];
+        outer_coefs<S>(tab, k, m, mp, c);
+        load((mp - m) * S::gs(k), y);
+        partner_mac(c, y, acc);
+      }
+    }
+    if (lane < rows) {
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const long long at = e * quarter + 4 * o;
+        float4 w0, w1;
+        w0.x = sf * acc[e][0].x;
+        w0.y = sf * acc[e][0].y;
+        w0.z = sf * acc[e][1].x;
+        w0.w = sf * acc[e][1].y;
+        w1.x = sf * acc[e][2].x;
+        w1.y = sf * acc[e][2].y;
+        w1.z = sf * acc[e][3].x;
+        w1.w = sf * acc[e][3].y;
+        *reinterpret_cast<float4*>(y_b + at) = w0;
+        *reinterpret_cast<float4*>(y_b + at + 2) = w1;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Pass L: every l x 16 columns (eB x 8 consecutive r) per CTA; lane bits 0-2
+// = r, bit 3 = eB, bit 4 = digit K-3 of l.  Cube = eA x digits K-2, K-1.
+// ---------------------------------------------------------------------------
+template <int N1, int NH>
+struct PassL {
+  using S = Shape<N1, NH>;
+  static constexpr int HL = S::HALF;
+  static constexpr int NO = HL / 8;  // outer indices
+  static constexpr int NL = 2 * HL;
+  static constexpr int TAB_BYTES = align16c(S::NTAB * 8);
+  static constexpr int OREC_BYTES = align16c(NO * (int)sizeof(ORec));
+  static constexpr int SMEM = TAB_BYTES + OREC_BYTES + NL * 16 * 8;
+  static constexpr int WARPS =
+      NO % 8 == 0 ? 8 : NO % 6 == 0 ? 6 : NO % 9 == 0 ? 9 : NO % 4 == 0 ? 4 : NO % 3 == 0 ? 3 : NO < 8 ? NO : 8;
+  static_assert(NH >= 3, "pass L needs three trailing spin-1/2 digits");
+};
+
+template <int N1, int NH>
+__global__ void __launch_bounds__(PassL<N1, NH>::WARPS * 32, 2)
+    fast_pass_l(HpsiArgs<float2> a, const float2* __restrict__ yb) {
+  using P = PassL<N1, NH>;
+  using S = typename P::S;
+  constexpr int K = S::K;
+  constexpr int HL = P::HL, NO = P::NO, NL = P::NL;
+  constexpr int NT = P::WARPS * 32;
+  const int b = gridDim.y - 1 - blockIdx.y;
+  if (skip_vec(a, b)) return;
+  const CubeView<float2>* view = a.views + (a.sys_of ? a.sys_of[b] : 0);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* tab = reinterpret_cast<float2*>(smem_raw);
+  ORec* orec = reinterpret_cast<ORec*>(smem_raw + P::TAB_BYTES);
+  float2* tile = reinterpret_cast<float2*>(smem_raw + P::TAB_BYTES + P::OREC_BYTES);
+  const int HR = view->half_r;
+  const long long quarter = (long long)HL * HR;
+  const int c0 = blockIdx.x * 8;
+  const float2* x_in = a.in + (long long)b * a.ld;
+  for (int idx = threadIdx.x; idx < NL * 8; idx += NT) {
+    const int l = idx >> 3, h = (idx >> 2) & 1, q = idx & 3;
+    const int ea = l >= HL ? 1 : 0;
+    const int llo = l - ea * HL;
+    copy16(tile + l * 16 + h * 8 + 2 * q, x_in + (2 * ea + h) * quarter + (long long)llo * HR + c0 + 2 * q);
+  }
+  for (int k = threadIdx.x; k < S::NTAB; k += NT) tab[k] = view->tabL[k];
+  __syncthreads();
+  for (int o = threadIdx.x; o < NO; o += NT) {
+    ORec r;
+    r.d[0] = tab[0].x;
+    r.d[1] = tab[1].x;
+    r.f[0] = tab[2];
+    r.f[1] = tab[3];
+#pragma unroll
+    for (int k = 0; k < K - 3; ++k) {
+      const int m = (o / (S::gs(k) / 8)) % S::dim(k);
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        r.d[e] += tab[S::offD(k) + e * S::dim(k) + m].x;
+        r.f[e] = cadd(r.f[e], tab[S::offF(k) + e * S::dim(k) + m]);
+      }
+    }
+    orec[o] = r;
+  }
+  copy_wait_all();
+  __syncthreads();
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int j = lane & 7, h = (lane >> 3) & 1, lg = lane >> 4, c = lane & 15;
+  const float sf = (float)in_scale(a, b);
+  // electron-pair operator rows of (e, h): eB-diagonal part merged, eB flip via the partner column
+  float dp[2];
+  float2 fp[2], pp[2][2];
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    dp[e] = view->pair[(e * 2 + h) * 4 + e * 2 + h].x;
+    fp[e] = view->pair[(e * 2 + h) * 4 + (1 - e) * 2 + h];
+#pragma unroll
+    for (int ep = 0; ep < 2; ++ep) pp[e][ep] = view->pair[(e * 2 + h) * 4 + ep * 2 + (1 - h)];
+  }
+  // lane digit K-3
+  float dL[2];
+  float2 fL[2], cL[2][2];
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    dL[e] = tab[S::offD(K - 3) + e * 2 + lg].x + dp[e];
+    fL[e] = cadd(tab[S::offF(K - 3) + e * 2 + lg], fp[e]);
+#pragma unroll
+    for (int ep = 0; ep < 2; ++ep) cL[e][ep] = tab[S::offX(K - 3) + (e * 2 + lg) * 4 + ep * 2 + (1 - lg)];
+  }
+  float din[2][4];
+  float2 fin[2][4];
+  cube_consts<S>(tab, din, fin);
+  const float2* col = tile + c;
+  const long long cofs = h * quarter + c0 + j;
+  const float2* y_b = yb + (long long)b * (a.ya_ld ? a.ya_ld : a.ld) + cofs;
+  float2* y_out = a.out + (long long)b * a.ld + cofs;
+  double dot = 0.0;
+  for (int o = warp; o < NO; o += P::WARPS) {
+    const ORec rec = orec[o];
+    const int lo = o * 8 + lg * 4;  // l of cube element i = 0
+    float2 pb[2][4];  // pass-R partial of the cube, loaded early to hide its latency
+#pragma unroll
+    for (int e = 0; e < 2; ++e)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) pb[e][i] = __ldcg(y_b + 2 * e * quarter + (long long)(lo + i) * HR);
+    float2 x[2][4], acc[2][4];
+#pragma unroll
+    for (int e = 0; e < 2; ++e)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) x[e][i] = col[(e * HL + lo + i) * 16];
+#pragma unroll
+    for (int e = 0; e < 2; ++e)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        acc[e][i] = rmacf(rec.d[e] + dL[e] + din[e][i], x[e][i], make_float2(0.f, 0.f));
+        acc[e][i] = cfma(cadd(cadd(rec.f[e], fL[e]), fin[e][i]), x[1 - e][i], acc[e][i]);
+      }
+    cube_inner<S>(tab, x, acc);
+    auto partner = [&](int delta, int dcol, const float2 (&cc)[2][2]) {
+      float2 y[2][4];
+#pragma unroll
+      for (int ep = 0; ep < 2; ++ep)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) y[ep][i] = tile[(ep * HL + lo + delta + i) * 16 + dcol];
+      partner_mac(cc, y, acc);
+    };
+    partner((1 - 2 * lg) * 4, c, cL);  // lane digit
+    partner(0, c ^ 8, pp);             // electron B flip (pair operator)
+#pragma unroll
+    for (int k = 0; k < K - 3; ++k) {
+      const int m = (o / (S::gs(k) / 8)) % S::dim(k);
+#pragma unroll
+      for (int t = 1; t < S::dim(k); ++t) {
+        const int mp = m + t >= S::dim(k) ? m + t - S::dim(k) : m + t;
+        float2 cc[2][2];
+        outer_coefs<S>(tab, k, m, mp, cc);
+        partner((mp - m) * S::gs(k), c, cc);
+      }
+    }
+    float part = 0.f;
+#pragma unroll
+    for (int e = 0; e < 2; ++e)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        float2 v;
+        v.x = fmaf(sf, acc[e][i].x, pb[e][i].x);
+        v.y = fmaf(sf, acc[e][i].y, pb[e][i].y);
+        y_out[2 * e * quarter + (long long)(lo + i) * HR] = v;
+        part = fmaf(x[e][i].x, v.x, fmaf(x[e][i].y, v.y, part));
+      }
+    dot += (double)part * (double)sf;
+  }
+  if (a.dot_part) finish_dot_fast(a, b, dot);
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+// Raise the dynamic shared-memory limit once per kernel and device, so that
+// launches recorded into a CUDA graph issue no attribute calls.
+template <class K>
+void set_smem(K kern, int bytes) {
+  static std::vector<std::pair<const void*, int>> done;  // (kernel, device)
+  int dev = 0;
+  check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+  const void* key = reinterpret_cast<const void*>(kern);
+  for (const auto& d : done)
+    if (d.first == key && d.second == dev) return;
+  check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes), "fast H psi smem attr");
+  done.emplace_back(key, dev);
+}
+
+template <int N1, int NH>
+void launch_l(const HpsiArgs<float2>& a, const float2* yb, int half_r, int batch, cudaStream_t st) {
+  using P = PassL<N1, NH>;
+  auto kern = fast_pass_l<N1, NH>;
+  set_smem(kern, P::SMEM);
+  kern<<<dim3(half_r / 8, batch), P::WARPS * 32, P::SMEM, st>>>(a, yb);
+  check_launch("fast_pass_l");
+}
+
+template <int N1, int NH>
+void launch_r(const HpsiArgs<float2>& a, float2* yb, int half_l, int batch, cudaStream_t st) {
+  using P = PassR<N1, NH>;
+  auto kern = fast_pass_r<N1, NH>;
+  set_smem(kern, P::SMEM);
+  kern<<<dim3((2 * half_l + 31) / 32, batch), P::WARPS * 32, P::SMEM, st>>>(a, yb);
+  check_launch("fast_pass_r");
+}
+
+using LaunchL = void (*)(const HpsiArgs<float2>&, const float2*, int, int, cudaStream_t);
+using LaunchR = void (*)(const HpsiArgs<float2>&, float2*, int, int, cudaStream_t);
+
+// Instantiated digit patterns (spin-1 count, spin-1/2 count) per radical.
+LaunchL pick_l(int n1, int nh) {
+  if (n1 == 2 && nh == 5) return launch_l<2, 5>;
+  if (n1 == 2 && nh == 3) return launch_l<2, 3>;
+  if (n1 == 2 && nh == 4) return launch_l<2, 4>;
+  if (n1 == 2 && nh == 6) return launch_l<2, 6>;
+  if (n1 == 1 && nh == 5) return launch_l<1, 5>;
+  if (n1 == 1 && nh == 6) return launch_l<1, 6>;
+  if (n1 == 0 && nh == 6) return launch_l<0, 6>;
+  return nullptr;
+}
+LaunchR pick_r(int n1, int nh) {
+  if (n1 == 1 && nh == 6) return launch_r<1, 6>;
+  if (n1 == 1 && nh == 4) return launch_r<1, 4>;
+  if (n1 == 1 && nh == 5) return launch_r<1, 5>;
+  if (n1 == 1 && nh == 3) return launch_r<1, 3>;
+  if (n1 == 1 && nh == 2) return launch_r<1, 2>;
+  if (n1 == 2 && nh == 5) return launch_r<2, 5>;
+  if (n1 == 0 && nh == 6) return launch_r<0, 6>;
+  return nullptr;
+}
+
+// (spin-1 count, spin-1/2 count) of a cube side when its digits are all
+// spin-1 first, then all spin-1/2; {-1, -1} otherwise.
+void side_pattern(const CubeSide& s, int& n1, int& nh) {
+  n1 = nh = 0;
+  int k = 0;
+  while (k < s.K && s.dim[k] == 3) ++k, ++n1;
+  while (k < s.K && s.dim[k] == 2) ++k, ++nh;
+  if (k != s.K) n1 = nh = -1;
+}
+
+}  // namespace
+
+// Fills the fast-path fields of `p` for one system (first == true) or checks
+// that another system of the same launch has the same shape.
+void fast_plan_add(CubePlan& p, const rpm_system* s, bool first) {
+  int n1l, nhl, n1r, nhr;
+  side_pattern(s->cube_l, n1l, nhl);
+  side_pattern(s->cube_r, n1r, nhr);
+  bool ok = s->cube && n1l >= 0 && n1r >= 0 && pick_l(n1l, nhl) && pick_r(n1r, nhr) && s->half_r % 8 == 0;
+  if (ok) {
+    // standard layout: offl[l] = eA * N/2 + l_lo * HR, offr[r] = eB * N/4 + r_lo
+    const long long n = s->n, hl = s->half_l, hr = s->half_r;
+    for (long long l = 0; ok && l < (long long)s->offl.size(); ++l)
+      ok = s->offl[l] == (l / hl) * (n / 2) + (l % hl) * hr;
+    for (long long r = 0; ok && r < (long long)s->offr.size(); ++r) ok = s->offr[r] == (r / hr) * (n / 4) + (r % hr);
+  }
+  if (first) {
+    p.fast = ok ? 1 : 0;
+    p.fl_n1 = n1l;
+    p.fl_nh = nhl;
+    p.fr_n1 = n1r;
+    p.fr_nh = nhr;
+    p.f_half_l = s->half_l;
+    p.f_half_r = s->half_r;
+  } else if (!ok || n1l != p.fl_n1 || nhl != p.fl_nh || n1r != p.fr_n1 || nhr != p.fr_nh || s->half_l != p.f_half_l ||
+             s->half_r != p.f_half_r) {
+    p.fast = 0;
+  }
+}
+
+bool launch_cube_fast(const HpsiArgs<float2>& a, const CubePlan& p, float2* ya, int batch, cudaStream_t st) {
+  if (!p.fast) return false;
+  const long long yld = a.ya_ld ? a.ya_ld : a.ld;
+  auto aligned = [](const void* ptr) { return (reinterpret_cast<uintptr_t>(ptr) & 15u) == 0; };
+  if ((a.ld & 1) || (yld & 1) || !aligned(a.in) || !aligned(a.out) || !aligned(ya)) return false;
+  const LaunchL fl = pick_l(p.fl_n1, p.fl_nh);
+  const LaunchR fr = pick_r(p.fr_n1, p.fr_nh);
+  if (!fl || !fr) return false;
+  HpsiArgs<float2> ar = a;
+  ar.dot_part = nullptr;
+  fr(ar, ya, p.f_half_l, batch, st);
+  fl(a, ya, p.f_half_r, batch, st);
+  return true;
+}
+
+}  // namespace rpm
+
+extern "C" int rpm_system_fast_hpsi(const rpm_system* sys, int* usable) {
+  return rpm::guarded([&] {
+    if (!sys || !usable) rpm::fail(RPM_E_INVALID, "NULL argument");
+    rpm::CubePlan p{};
+    if (sys->split && sys->cube) rpm::fast_plan_add(p, sys, true);
+    *usable = p.fast;
+  });
+}

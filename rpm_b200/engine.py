@@ -106,6 +106,13 @@ class _DeviceSystem:
         _lib.call("rpm_system_info", handle, *[ctypes.byref(v) for v in info])
         self.n, self.split, self.nl, self.nr, self.nnz_l, self.nnz_r = (v.value for v in info)
 
+    @property
+    def fast_hpsi(self) -> bool:
+        """True when complex64 H psi runs on the shape-specialised kernels."""
+        flag = ctypes.c_int(0)
+        _lib.call("rpm_system_fast_hpsi", self.handle, ctypes.byref(flag))
+        return bool(flag.value)
+
     def split_tables(self):
         nl, nr = self.nl, self.nr
         lptr, rptr = np.zeros(nl + 1, np.int32), np.zeros(nr + 1, np.int32)
