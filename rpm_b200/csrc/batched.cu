@@ -397,57 +397,115 @@ __global__ void __launch_bounds__(kEwThreads) k_b_rebuild(BatchDev B) {
 }
 
 // Singlet Gram partials  G_kl = sum_q conj(a_k(q)) a_l(q),
-// a_k(q) = (V_k[n/4 + q] - V_k[n/2 + q]) / sqrt 2, FP32 within a row chunk and
-// FP64 across chunks.
-constexpr int kGramChunk = 32;
+// a_k(q) = (V_k[n/4 + q] - V_k[n/2 + q]) / sqrt 2, over this block's rows.
+// Register-tiled: thread (u, g) owns the 4x4 tile u of the upper triangle
+// (tile row <= tile column; the Hermitian lower half is written mirrored)
+// for the rows g, g + NG, ... of each staged chunk.  Products and sums are
+// FP32 within one chunk and FP64 across chunks and row groups.
+constexpr int kGramChunk = 64;   // rows per staged chunk
+constexpr int kGramGroups = 8;   // at most this many row groups per block
 __global__ void __launch_bounds__(256) k_b_gram(BatchDev B) {
-  __shared__ float2 a[kGramChunk * kBMaxK];
+  // staged chunk; reused for the row-group sum (needed only when NG > 1,
+  // i.e. at most 128 tiles: 16 x 128 double2 = 32 KiB <= the chunk's bytes)
+  __shared__ __align__(16) float2 a[kGramChunk][kBMaxK + 2];
+  double2(*red)[128] = reinterpret_cast<double2(*)[128]>(&a[0][0]);
+  static_assert(sizeof(a) >= 16 * 128 * sizeof(double2), "row-group buffer does not fit");
   const int b = blockIdx.y;
   TrajState& s = B.st[b];
   if (s.done) return;
   const int M = s.msize;
+  const int T = (M + 3) / 4;             // tiles per side
+  const int NU = T * (T + 1) / 2;        // upper-triangle tiles
+  const int NG = min(kGramGroups, max(1, (int)blockDim.x / NU));
+  const int u = threadIdx.x % NU, g = threadIdx.x / NU;
+  const bool worker = g < NG;
+  int ti = 0, rem = u;
+  while (rem >= T - ti) {
+    rem -= T - ti;
+    ++ti;
+  }
+  const int tj = ti + rem;
   const long long q4 = s.n / 4;
   const float2* V = B.V + (size_t)b * (B.m + 1) * B.ld;
-  const int pairs = M * M;
-  double2 acc[16];
-#pragma unroll
-  for (int p = 0; p < 16; ++p) acc[p] = make_double2(0.0, 0.0);
   const float rs2 = 0.70710678118654752440f;
+  double2 acc[4][4];
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[p][q] = make_double2(0.0, 0.0);
+  const int KP = 4 * T;  // staged columns (zero beyond M)
   for (long long r0 = (long long)blockIdx.x * kGramChunk; r0 < q4; r0 += (long long)gridDim.x * kGramChunk) {
     __syncthreads();
-    for (int idx = threadIdx.x; idx < kGramChunk * M; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < kGramChunk * KP; idx += blockDim.x) {
       const int k = idx / kGramChunk, rr = idx % kGramChunk;
       const long long qq = r0 + rr;
       float2 v = make_float2(0.f, 0.f);
-      if (qq < q4) {
+      if (qq < q4 && k < M) {
         const float2 p1 = V[(size_t)k * B.ld + q4 + qq];
         const float2 p2 = V[(size_t)k * B.ld + 2 * q4 + qq];
         v = make_float2((p1.x - p2.x) * rs2, (p1.y - p2.y) * rs2);
       }
-      a[rr * kBMaxK + k] = v;
+      a[rr][k] = v;
     }
     __syncthreads();
+    if (worker) {
+      float2 cs[4][4];
 #pragma unroll
-    for (int p = 0; p < 16; ++p) {
-      const int pr = threadIdx.x + p * blockDim.x;
-      if (pr < pairs) {
-        const int k = pr / M, l = pr % M;
-        float sx = 0.f, sy = 0.f;
-        for (int rr = 0; rr < kGramChunk; ++rr) {
-          const float2 u = a[rr * kBMaxK + k], v = a[rr * kBMaxK + l];
-          sx = fmaf(u.x, v.x, fmaf(u.y, v.y, sx));
-          sy = fmaf(u.x, v.y, fmaf(-u.y, v.x, sy));
-        }
-        acc[p].x += sx;
-        acc[p].y += sy;
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) cs[p][q] = make_float2(0.f, 0.f);
+      for (int rr = g; rr < kGramChunk; rr += NG) {
+        const float4 u01 = *reinterpret_cast<const float4*>(&a[rr][4 * ti]);
+        const float4 u23 = *reinterpret_cast<const float4*>(&a[rr][4 * ti + 2]);
+        const float4 v01 = *reinterpret_cast<const float4*>(&a[rr][4 * tj]);
+        const float4 v23 = *reinterpret_cast<const float4*>(&a[rr][4 * tj + 2]);
+        const float2 uu[4] = {make_float2(u01.x, u01.y), make_float2(u01.z, u01.w), make_float2(u23.x, u23.y),
+                              make_float2(u23.z, u23.w)};
+        const float2 vv[4] = {make_float2(v01.x, v01.y), make_float2(v01.z, v01.w), make_float2(v23.x, v23.y),
+                              make_float2(v23.z, v23.w)};
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            cs[p][q].x = fmaf(uu[p].x, vv[q].x, fmaf(uu[p].y, vv[q].y, cs[p][q].x));
+            cs[p][q].y = fmaf(uu[p].x, vv[q].y, fmaf(-uu[p].y, vv[q].x, cs[p][q].y));
+          }
       }
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          acc[p][q].x += cs[p][q].x;
+          acc[p][q].y += cs[p][q].y;
+        }
     }
   }
-  double2* out = B.gpart + ((size_t)b * B.gblk + blockIdx.x) * kBMaxK * kBMaxK;
+  // sum the row groups in FP64, one group at a time (NG > 1 implies NU <= 128)
+  if (NG > 1) {
+    __syncthreads();  // the chunk buffer is reused
+    for (int gg = 0; gg < NG; ++gg) {
+      if (worker && g == gg) {
 #pragma unroll
-  for (int p = 0; p < 16; ++p) {
-    const int pr = threadIdx.x + p * blockDim.x;
-    if (pr < pairs) out[pr] = acc[p];
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) red[p * 4 + q][u] = gg ? cadd(red[p * 4 + q][u], acc[p][q]) : acc[p][q];
+      }
+      __syncthreads();
+    }
+  }
+  double2* out = B.gpart + ((size_t)b * B.gblk + blockIdx.x) * kBMaxK * kBMaxK;  // compact M x M
+  if (worker && g == 0) {
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int k = 4 * ti + p, l = 4 * tj + q;
+        if (k < M && l < M) {
+          const double2 v = NG > 1 ? red[p * 4 + q][u] : acc[p][q];
+          out[k * M + l] = v;
+          if (ti != tj) out[l * M + k] = make_double2(v.x, -v.y);
+        }
+      }
   }
 }
 
@@ -541,6 +599,7 @@ struct rpm_batch {
   long long probe_samples = 0;
   long long kernel_launches = 0, replays = 0;
   int launches_per_step = 0;
+  bool fused = false;  // Lanczos recurrence fused into the H psi passes
 };
 
 namespace rpm {
@@ -606,17 +665,45 @@ static void record_step(rpm_batch* Bh, const BatchDev& B, const Layout& L, cudaS
   cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
   check_cuda(cudaStreamIsCapturing(st, &capturing), "capture status");
   const unsigned probe_flags = capturing == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : 0u;
+  // The shape-specialised passes carry the Lanczos recurrence themselves
+  // (LanczosFuse: no update kernel); otherwise H psi + k_b_update.
+  a.in = B.V;
+  a.out = B.V + B.ld;
+  const bool fused = cube_fast_usable(a, Bh->plan, ya);
   for (int j = 0; j < m; ++j) {
     a.in = B.V + (size_t)j * B.ld;
     a.out = B.V + (size_t)(j + 1) * B.ld;
-    a.dot_out = &B.st[0].alpha[j];
     // While capturing, external records become event-record nodes of the graph.
     if (j == probe_j) check_cuda(cudaEventRecordWithFlags(Bh->probe0, st, probe_flags), "probe record");
-    launch_cube<float2>(a, Bh->plan, ya, B.ntraj, st);
+    if (fused) {
+      LanczosFuse& z = a.lz;
+      z.on = 1;
+      z.first = j == 0;
+      z.last = j == m - 1;
+      z.j = j;
+      z.prev = j > 0 ? B.V + (size_t)(j - 1) * B.ld : nullptr;
+      z.alpha_prev = j > 0 ? &B.st[0].alpha[j - 1] : nullptr;
+      z.beta_prev = j > 0 ? &B.st[0].beta[j - 1] : nullptr;
+      z.alpha_out = &B.st[0].alpha[j];
+      z.beta_out = &B.st[0].beta[j];
+      z.scale_out = &B.st[0].scale;
+      z.stop = &B.st[0].stop;
+      z.skip = &B.st[0].skip;
+      z.msize = &B.st[0].msize;
+      z.dstride = kStateDoubles;
+      z.istride = kStateInts;
+      z.breakdown_rel = B.breakdown_rel;
+      a.dot_out = nullptr;
+      if (!launch_cube_fast(a, Bh->plan, ya, B.ntraj, st)) fail(RPM_E_INVALID, "fused Lanczos passes unavailable");
+    } else {
+      a.dot_out = &B.st[0].alpha[j];
+      launch_cube<float2>(a, Bh->plan, ya, B.ntraj, st);
+    }
     if (j == probe_j) check_cuda(cudaEventRecordWithFlags(Bh->probe1, st, probe_flags), "probe record");
-    k_b_update<<<ew, kEwThreads, 0, st>>>(B, j);
+    if (!fused) k_b_update<<<ew, kEwThreads, 0, st>>>(B, j);
   }
-  Bh->launches_per_step = 1 + 3 * m + 4;
+  Bh->fused = fused;
+  Bh->launches_per_step = 1 + (fused ? 2 : 3) * m + 4;
   const size_t ctl_smem = sizeof(double) * 2 * kRecDoubles;
   k_b_control<<<B.ntraj, 128, ctl_smem, st>>>(B);
   k_b_rebuild<<<ew, kEwThreads, 0, st>>>(B);

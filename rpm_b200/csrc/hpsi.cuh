@@ -5,6 +5,32 @@
 
 namespace rpm {
 
+// Fused Lanczos recurrence of the shape-specialised complex64 passes (off
+// when `on` is 0).  Iteration j of vector b, in Paige's ordering:
+//   pass R stages v_j = (w'_j - alpha_{j-1} v_{j-1}) * in_scale (j > 0) from
+//          `in` (holding w'_j) and `prev`, and writes v_j back into `in`;
+//   pass L writes w'_{j+1} = H v_j - beta_{j-1} v_{j-1} into `out` (not for
+//          the last iteration) and reduces <v_j, w'>, |w'|^2 and |v_j|^2;
+//          its last block sets alpha_j = <v_j, w'> / |v_j|^2 and
+//          beta_j = |w' - alpha_j v_j|, scale = 1 / beta_j, and flags a
+//          breakdown (beta_j <= breakdown_rel (|alpha_j| + beta_{j-1})).
+// Per-vector scalars of vector b live at ptr + b * dstride (doubles) or
+// ptr + b * istride (ints).
+struct LanczosFuse {
+  int on, first, last, j;
+  const float2* prev;  // v_{j-1} of vector b at prev + b * ld (unused when first)
+  const double* alpha_prev;
+  const double* beta_prev;
+  double* alpha_out;
+  double* beta_out;
+  double* scale_out;
+  int* stop;
+  int* skip;
+  int* msize;
+  int dstride, istride;
+  double breakdown_rel;
+};
+
 // Arguments of one batched H psi launch.  Vector b of the batch is read from
 // in + b*ld and written to out + b*ld; everything else is optional.
 template <class T>
@@ -22,8 +48,9 @@ struct HpsiArgs {
   // fused <in_scaled, H in_scaled> of vector b into dot_out[b*dot_stride]
   double* dot_out;
   int dot_stride;
-  double* dot_part;     // gridDim.x partials per vector
+  double* dot_part;     // gridDim.x partials per vector (three per block with `lz`)
   unsigned* dot_count;  // one completion counter per vector (zero on entry)
+  LanczosFuse lz;       // complex64 shape-specialised passes only
 };
 
 // Shape limits of one launch over one or more systems.
@@ -44,6 +71,7 @@ void fast_plan_add(CubePlan& p, const rpm_system* s, bool first);
 // Launches the specialised passes; false (nothing launched) when the plan or
 // the pointers/strides (16-byte alignment) do not allow them.
 bool launch_cube_fast(const HpsiArgs<float2>& a, const CubePlan& p, float2* ya, int batch, cudaStream_t stream);
+bool cube_fast_usable(const HpsiArgs<float2>& a, const CubePlan& p, const float2* ya);
 // Two passes: pass L into `ya` (batch x ld scratch), pass R into a.out.
 template <class T>
 void launch_cube(const HpsiArgs<T>& a, const CubePlan& p, T* ya, int batch, cudaStream_t stream);

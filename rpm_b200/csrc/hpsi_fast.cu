@@ -118,6 +118,65 @@ __device__ void finish_dot_fast(const HpsiArgs<float2>& a, int b, double mine) {
   }
 }
 
+// Fused Lanczos reductions (s0 = <v_j, w'>, s1 = |w'|^2, s2 = |v_j|^2): per
+// block partials, then the last block of vector b sums them in block order
+// and sets alpha_j, beta_j, the scale and the breakdown flags (LanczosFuse).
+__device__ void finish_lanczos(const HpsiArgs<float2>& a, int b, double s0, double s1, double s2) {
+  __shared__ double red[3][32];
+  __shared__ bool last;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = s0;
+    red[1][threadIdx.x >> 5] = s1;
+    red[2][threadIdx.x >> 5] = s2;
+  }
+  __syncthreads();
+  double* part = a.dot_part + (long long)b * gridDim.x * 3;
+  if (threadIdx.x == 0) {
+    double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      t0 += red[0][w];
+      t1 += red[1][w];
+      t2 += red[2][w];
+    }
+    part[blockIdx.x * 3 + 0] = t0;
+    part[blockIdx.x * 3 + 1] = t1;
+    part[blockIdx.x * 3 + 2] = t2;
+    __threadfence();
+    last = atomicAdd(a.dot_count + b, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+    for (int k = 0; k < (int)gridDim.x; ++k) {
+      t0 += __ldcg(part + 3 * k);
+      t1 += __ldcg(part + 3 * k + 1);
+      t2 += __ldcg(part + 3 * k + 2);
+    }
+    const LanczosFuse& z = a.lz;
+    const double alpha = t2 > 0.0 ? t0 / t2 : 0.0;
+    z.alpha_out[(long long)b * z.dstride] = alpha;
+    if (!z.last) {
+      const double beta = sqrt(fmax(t1 - t0 * alpha, 0.0));  // |w' - alpha v_j|
+      z.beta_out[(long long)b * z.dstride] = beta;
+      z.scale_out[(long long)b * z.dstride] = beta > 0.0 ? 1.0 / beta : 0.0;
+      const double ref = fabs(alpha) + (z.first ? 0.0 : z.beta_prev[(long long)b * z.dstride]);
+      if (!(beta > z.breakdown_rel * ref)) {
+        z.stop[(long long)b * z.istride] = 1;
+        z.skip[(long long)b * z.istride] = 1;
+        z.msize[(long long)b * z.istride] = z.j + 1;
+      }
+    }
+    a.dot_count[b] = 0;
+  }
+}
+
 // Merged diagonal / flip coefficients of the two register-cube digits
 // (digits K-2 -> bit 1 of i, K-1 -> bit 0 of i).
 template <class S>
@@ -214,13 +273,60 @@ __global__ void __launch_bounds__(PassR<N1, NH>::WARPS * 32, 2)
   const long long quarter = (long long)half_l * HR;
   const float2* x_in = a.in + (long long)b * a.ld;
   constexpr int CH = HR / 2;  // 16-byte chunks per half row
-  for (int idx = threadIdx.x; idx < rows * 2 * CH; idx += NT) {
+  const int units = rows * 2 * CH;
+  auto unit_at = [&](int idx, int& slot, long long& g) {
     const int rr = idx / (2 * CH), rem = idx - rr * (2 * CH);
     const int e = rem / CH, c = rem - e * CH;
     const int rho = row0 + rr;
     const int ea = rho >= half_l ? 1 : 0;
     const int llo = rho - ea * half_l;
-    copy16(tile + rr * RS + e * HR + 2 * c, x_in + (2 * ea + e) * quarter + (long long)llo * HR + 2 * c);
+    slot = rr * RS + e * HR + 2 * c;
+    g = (2 * ea + e) * quarter + (long long)llo * HR + 2 * c;
+  };
+  if (a.lz.on && !a.lz.first) {
+    // v_j = (w'_j - alpha_{j-1} v_{j-1}) * scale, staged and written back into `in`
+    const float al = (float)a.lz.alpha_prev[(long long)b * a.lz.dstride];
+    const float sc = (float)in_scale(a, b);
+    const float2* pv = a.lz.prev + (long long)b * a.ld;
+    float2* xo = const_cast<float2*>(x_in);
+    constexpr int UB = 6;  // units per thread in flight
+    for (int base = threadIdx.x; base < units; base += NT * UB) {
+      float4 w[UB], q[UB];
+#pragma unroll
+      for (int u = 0; u < UB; ++u) {
+        const int idx = base + u * NT;
+        if (idx < units) {
+          int slot;
+          long long g;
+          unit_at(idx, slot, g);
+          w[u] = __ldcg(reinterpret_cast<const float4*>(x_in + g));
+          q[u] = __ldcg(reinterpret_cast<const float4*>(pv + g));
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < UB; ++u) {
+        const int idx = base + u * NT;
+        if (idx < units) {
+          int slot;
+          long long g;
+          unit_at(idx, slot, g);
+          float4 v;
+          v.x = sc * fmaf(-al, q[u].x, w[u].x);
+          v.y = sc * fmaf(-al, q[u].y, w[u].y);
+          v.z = sc * fmaf(-al, q[u].z, w[u].z);
+          v.w = sc * fmaf(-al, q[u].w, w[u].w);
+          *reinterpret_cast<float4*>(tile + slot) = v;
+          *reinterpret_cast<float4*>(xo + g) = v;
+        }
+      }
+    }
+  } else {
+    for (int idx = threadIdx.x; idx < units; idx += NT) {
+      int slot;
+      long long g;
+      unit_at(idx, slot, g);
+      copy16(tile + slot, x_in + g);
+    }
   }
   for (int k = threadIdx.x; k < S::NTAB; k += NT) tab[k] = view->tabR[k];
   __syncthreads();
@@ -245,7 +351,7 @@ __global__ void __launch_bounds__(PassR<N1, NH>::WARPS * 32, 2)
   __syncthreads();
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const float sf = (float)in_scale(a, b);
+  const float sf = a.lz.on ? 1.0f : (float)in_scale(a, b);  // fused: the staged v_j is already scaled
   const float2* rowp = tile + lane * RS;
   float din[2][4];
   float2 fin[2][4];
@@ -376,7 +482,11 @@ __global__ void __launch_bounds__(PassL<N1, NH>::WARPS * 32, 2)
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int j = lane & 7, h = (lane >> 3) & 1, lg = lane >> 4, c = lane & 15;
-  const float sf = (float)in_scale(a, b);
+  const bool fused = a.lz.on != 0;
+  const bool has_prev = fused && !a.lz.first;
+  const bool store = !fused || !a.lz.last;
+  const float sf = fused ? 1.0f : (float)in_scale(a, b);  // fused: pass R wrote the scaled v_j
+  const float bprev = has_prev ? (float)a.lz.beta_prev[(long long)b * a.lz.dstride] : 0.0f;
   // electron-pair operator rows of (e, h): eB-diagonal part merged, eB flip via the partner column
   float dp[2];
   float2 fp[2], pp[2][2];
@@ -404,15 +514,19 @@ __global__ void __launch_bounds__(PassL<N1, NH>::WARPS * 32, 2)
   const long long cofs = h * quarter + c0 + j;
   const float2* y_b = yb + (long long)b * (a.ya_ld ? a.ya_ld : a.ld) + cofs;
   float2* y_out = a.out + (long long)b * a.ld + cofs;
-  double dot = 0.0;
+  const float2* y_p = has_prev ? a.lz.prev + (long long)b * a.ld + cofs : nullptr;
+  double dot = 0.0, nw = 0.0, nv = 0.0;
   for (int o = warp; o < NO; o += P::WARPS) {
     const ORec rec = orec[o];
     const int lo = o * 8 + lg * 4;  // l of cube element i = 0
-    float2 pb[2][4];  // pass-R partial of the cube, loaded early to hide its latency
+    float2 pb[2][4], pp4[2][4];  // pass-R partial and v_{j-1} of the cube, loaded early
 #pragma unroll
     for (int e = 0; e < 2; ++e)
 #pragma unroll
-      for (int i = 0; i < 4; ++i) pb[e][i] = __ldcg(y_b + 2 * e * quarter + (long long)(lo + i) * HR);
+      for (int i = 0; i < 4; ++i) {
+        pb[e][i] = __ldcg(y_b + 2 * e * quarter + (long long)(lo + i) * HR);
+        pp4[e][i] = has_prev ? __ldcg(y_p + 2 * e * quarter + (long long)(lo + i) * HR) : make_float2(0.f, 0.f);
+      }
     float2 x[2][4], acc[2][4];
 #pragma unroll
     for (int e = 0; e < 2; ++e)
@@ -447,7 +561,7 @@ __global__ void __launch_bounds__(PassL<N1, NH>::WARPS * 32, 2)
         partner((mp - m) * S::gs(k), c, cc);
       }
     }
-    float part = 0.f;
+    float part = 0.f, pw = 0.f, px = 0.f;
 #pragma unroll
     for (int e = 0; e < 2; ++e)
 #pragma unroll
@@ -455,12 +569,21 @@ __global__ void __launch_bounds__(PassL<N1, NH>::WARPS * 32, 2)
         float2 v;
         v.x = fmaf(sf, acc[e][i].x, pb[e][i].x);
         v.y = fmaf(sf, acc[e][i].y, pb[e][i].y);
-        y_out[2 * e * quarter + (long long)(lo + i) * HR] = v;
+        if (has_prev) {  // Paige: w' = H v_j - beta_{j-1} v_{j-1}
+          v.x = fmaf(-bprev, pp4[e][i].x, v.x);
+          v.y = fmaf(-bprev, pp4[e][i].y, v.y);
+        }
+        if (store) y_out[2 * e * quarter + (long long)(lo + i) * HR] = v;
         part = fmaf(x[e][i].x, v.x, fmaf(x[e][i].y, v.y, part));
+        pw = fmaf(v.x, v.x, fmaf(v.y, v.y, pw));
+        px = fmaf(x[e][i].x, x[e][i].x, fmaf(x[e][i].y, x[e][i].y, px));
       }
     dot += (double)part * (double)sf;
+    nw += (double)pw;
+    nv += (double)px;
   }
-  if (a.dot_part) finish_dot_fast(a, b, dot);
+  if (fused) finish_lanczos(a, b, dot, nw, nv);
+  else if (a.dot_part) finish_dot_fast(a, b, dot);
 }
 
 // ---------------------------------------------------------------------------
@@ -563,14 +686,19 @@ void fast_plan_add(CubePlan& p, const rpm_system* s, bool first) {
   }
 }
 
-bool launch_cube_fast(const HpsiArgs<float2>& a, const CubePlan& p, float2* ya, int batch, cudaStream_t st) {
+bool cube_fast_usable(const HpsiArgs<float2>& a, const CubePlan& p, const float2* ya) {
   if (!p.fast) return false;
   const long long yld = a.ya_ld ? a.ya_ld : a.ld;
   auto aligned = [](const void* ptr) { return (reinterpret_cast<uintptr_t>(ptr) & 15u) == 0; };
   if ((a.ld & 1) || (yld & 1) || !aligned(a.in) || !aligned(a.out) || !aligned(ya)) return false;
+  if (a.lz.on && !a.lz.first && !aligned(a.lz.prev)) return false;
+  return pick_l(p.fl_n1, p.fl_nh) && pick_r(p.fr_n1, p.fr_nh);
+}
+
+bool launch_cube_fast(const HpsiArgs<float2>& a, const CubePlan& p, float2* ya, int batch, cudaStream_t st) {
+  if (!cube_fast_usable(a, p, ya)) return false;
   const LaunchL fl = pick_l(p.fl_n1, p.fl_nh);
   const LaunchR fr = pick_r(p.fr_n1, p.fr_nh);
-  if (!fl || !fr) return false;
   HpsiArgs<float2> ar = a;
   ar.dot_part = nullptr;
   fr(ar, ya, p.f_half_l, batch, st);
