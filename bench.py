@@ -168,10 +168,12 @@ def measured_peak_hbm():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def ncu_traffic_per_vector():
-    """DRAM bytes per vector of one batched H psi (both passes) from the
-    committed ncu summary, or None."""
-    path = ROOT / "profiles" / "hpsi_cube_c64_batched.md"
+def ncu_traffic_per_vector(fused: bool):
+    """DRAM bytes per vector of the dominant launch pair (one fused Lanczos
+    iteration, or one H psi for the general cube kernels) from the committed
+    ncu summary, or None."""
+    name = "lanczos_iteration_fused_c64.md" if fused else "hpsi_cube_c64_batched.md"
+    path = ROOT / "profiles" / name
     try:
         for line in path.read_text().splitlines():
             if line.startswith("dram_bytes_per_vector:"):
@@ -275,7 +277,7 @@ def b200_arm(args, rank: int, world: int, dist) -> None:
     vecs = synthetic.random_phase_vectors(full.dimensions, nvec, seed)
     states = np.stack([vecs[v] for k in range(args.orientations) for v in range(nvec)])
     system_index = np.array([k for k in range(args.orientations) for _ in range(nvec)], dtype=np.int32)
-    times = np.arange(int(round(HORIZON_US / GRID_US)) + 1) * GRID_US
+    times = np.arange(int(round(args.horizon / GRID_US)) + 1) * GRID_US
     bp = BatchedPropagator(hams, krylov_dimension=args.krylov, state_error_budget=args.budget)
     ld = bp.leading_dimension
     pristine = torch.zeros((ntraj, ld), dtype=torch.complex128, device=dev)
@@ -338,18 +340,24 @@ def b200_arm(args, rank: int, world: int, dist) -> None:
 
     line = None
     if rank == 0:
-        # roofline of the dominant kernel: one batched H psi (pass L + pass R)
+        # roofline of the dominant kernel pair, timed live on iteration 1 of
+        # every Krylov step: with the shape-specialised passes one fused
+        # Lanczos iteration (read w'_j and v_{j-1}, write v_j and w'_{j+1}:
+        # 32 N bytes per vector), else one H psi (read psi, write H psi: 16 N)
+        fused = bool(hams[0]._system.fast_hpsi)
         peak, peak_src = measured_peak_hbm()
         hpsi_s = counters["hpsi_ms"] / 1e3
-        alg_bytes = 16.0 * n * ntraj
+        alg_bytes = (32.0 if fused else 16.0) * n * ntraj
         achieved = alg_bytes / hpsi_s / 1e9 if hpsi_s > 0 else None
-        per_vec = ncu_traffic_per_vector()
+        per_vec = ncu_traffic_per_vector(fused)
+        kernel = ("fast_pass_r + fast_pass_l (one fused Lanczos iteration: complex64 H psi + Paige 3-term "
+                  "recurrence, all trajectories)" if fused else
+                  "cube_pass_l + cube_pass_r (complex64 H psi, one batched launch pair)")
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak if achieved else None,
                     "traffic": per_vec * ntraj if per_vec is not None else None,
                     "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured" else "fallback",
-                    "kernel": "cube_pass_l + cube_pass_r (complex64 H psi, one batched launch pair)",
-                    "algorithmic_bytes": alg_bytes, "avg_launch_ms": counters["hpsi_ms"],
+                    "kernel": kernel, "algorithmic_bytes": alg_bytes, "avg_launch_ms": counters["hpsi_ms"],
                     "samples": counters["hpsi_samples"]}
         # plain single-vector FP64 GPU path on trajectory 0 (same state and system)
         plain, y_err = None, None
@@ -362,7 +370,8 @@ def b200_arm(args, rank: int, world: int, dist) -> None:
             plain_s = time.perf_counter() - t0
             y_plain = rb.integrate_yield(times, ref.observable_values, LIFETIME_US)
             y_err = abs(float(yields[0].item()) - y_plain)
-            plain = {"value": 1.0 / plain_s, "unit": UNIT, "sample": "1 trajectory (orientation 0, vector 0), 5 us",
+            plain = {"value": 1.0 / plain_s, "unit": UNIT,
+                     "sample": f"1 trajectory (orientation 0, vector 0), {args.horizon:g} us",
                      "matvecs": ref.stats.matvecs, "krylov": "8-40", "budget": 1e-10}
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
@@ -378,8 +387,8 @@ def b200_arm(args, rank: int, world: int, dist) -> None:
             "scaling": "weak", "vs_baseline": None, "dtype": "c64 H-psi/basis + f64 Krylov control", "data": "synthetic",
             "config": {"workload": f"batched mixed-precision propagation, 221,184-dim synthetic FAD-TrpH-shaped radical "
                                    f"pair (2 e + 11 spin-1/2 + 3 spin-1), {args.orientations} Fibonacci field "
-                                   f"orientations x {nvec} random-phase vectors per GPU per step, 5 us, "
-                                   f"0.00125-us grid (4001 points), singlet yield tau = 1 us",
+                                   f"orientations x {nvec} random-phase vectors per GPU per step, {args.horizon:g} us, "
+                                   f"0.00125-us grid ({len(times)} points), singlet yield tau = 1 us",
                        "trajectories_per_step_per_gpu": ntraj, "krylov_dim": args.krylov,
                        "state_error_budget": args.budget, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (Krylov basis " f"{ntraj * (args.krylov + 1) * n * 8 / 1e9:.1f} GB)"},
@@ -412,6 +421,8 @@ def main() -> None:
     p.add_argument("--cpu-horizon", type=float, default=0.025, help="us of the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison trajectory")
+    p.add_argument("--horizon", type=float, default=HORIZON_US,
+                   help="propagation horizon in us (5 us is the benchmark workload; shorter only for profiling)")
     p.add_argument("--hpsi-only", type=int, default=0, metavar="K",
                    help="diagnostic: time K complex64 H psi launches over orientations x vectors states and exit")
     args = p.parse_args()

@@ -244,120 +244,284 @@ __global__ void __launch_bounds__(kEwThreads) k_b_update(BatchDev B, int j) {
   }
 }
 
-// Embedded error of the step dt; `c` receives c_hi(dt) (m entries).
-__device__ double step_error(const double* rec_hi, const double* rec_lo, bool exact, double dt, double safety,
-                             double norm, double2* ph, double2* c, double2* clo, double* red) {
-  spectral_coefficients<kBMaxK>(rec_hi, dt, ph, c);
-  if (exact) return 0.0;
-  spectral_coefficients<kBMaxK>(rec_lo, dt, ph, clo);
-  const int mh = (int)rec_hi[0], ml = (int)rec_lo[0];
-  double acc = 0.0;
-  for (int i = threadIdx.x; i < mh; i += blockDim.x) {
-    double2 d = c[i];
-    if (i < ml) {
-      d.x -= clo[i].x;
-      d.y -= clo[i].y;
-    }
-    acc = fma(d.x, d.x, fma(d.y, d.y, acc));
+// ---------------------------------------------------------------------------
+// Per-trajectory controller (one CTA of four warps per trajectory)
+// ---------------------------------------------------------------------------
+// Implicit symmetric tridiagonal QR with Wilkinson shifts (Golub & Van Loan,
+// section 8.3) run by ONE warp: lane 0 deflates and chases the bulge, every
+// lane applies the sweep's rotations to its rows of the eigenvector matrix.
+// Rotations are normalised with rsqrt instead of hypot and two divisions
+// (magnitudes here are far from the overflow range).  d, e: diagonal and
+// off-diagonal (d -> eigenvalues); z: m x m, row i = component i, leading
+// dimension ldz.  Returns 0 on convergence.
+__device__ int tridiag_qr_warp(int m, double* d, double* e, double* z, int ldz, double2* rot) {
+  const int lane = threadIdx.x & 31;
+  for (int idx = lane; idx < m * m; idx += 32) {
+    const int i = idx / m, k = idx - i * m;
+    z[i * ldz + k] = (i == k) ? 1.0 : 0.0;
   }
-  acc = block_sum(acc, red);
-  return safety * norm * sqrt(acc);
+  __syncwarp();
+  int sweeps = 0;
+  while (true) {
+    int p = 0, q = 0, state = 0;
+    if (lane == 0) {
+      for (int i = 0; i + 1 < m; ++i)
+        if (fabs(e[i]) <= DBL_EPSILON * (fabs(d[i]) + fabs(d[i + 1])) || fabs(e[i]) < DBL_MIN) e[i] = 0.0;
+      q = m - 1;
+      while (q > 0 && e[q - 1] == 0.0) --q;
+      if (q == 0) {
+        state = 1;
+      } else if (++sweeps > 40 * m) {
+        state = 2;
+      } else {
+        p = q - 1;
+        while (p > 0 && e[p - 1] != 0.0) --p;
+        const double delta = 0.5 * (d[q - 1] - d[q]);
+        const double eq = e[q - 1];
+        const double denom = delta + copysign(hypot(delta, eq), delta);
+        const double mu = d[q] - eq * eq / denom;
+        double x = d[p] - mu, y = e[p];
+        for (int k = p; k < q; ++k) {
+          double c = 1.0, sn = 0.0, r = 0.0;
+          const double rr = fma(x, x, y * y);
+          if (rr > 0.0) {
+            const double inv = rsqrt(rr);
+            c = x * inv;
+            sn = y * inv;
+            r = rr * inv;
+          }
+          if (k > p) e[k - 1] = r;
+          const double a = d[k], bb = e[k], cc = d[k + 1];
+          d[k] = c * c * a + 2.0 * c * sn * bb + sn * sn * cc;
+          d[k + 1] = sn * sn * a - 2.0 * c * sn * bb + c * c * cc;
+          e[k] = c * sn * (cc - a) + (c * c - sn * sn) * bb;
+          if (k + 1 < q) {
+            x = e[k];
+            y = sn * e[k + 1];
+            e[k + 1] = c * e[k + 1];
+          }
+          rot[k] = make_double2(c, sn);
+        }
+      }
+    }
+    state = __shfl_sync(0xffffffffu, state, 0);
+    p = __shfl_sync(0xffffffffu, p, 0);
+    q = __shfl_sync(0xffffffffu, q, 0);
+    __syncwarp();
+    if (state != 0) return state == 1 ? 0 : 1;
+    for (int i = lane; i < m; i += 32) {
+      double* row = z + i * ldz;
+      double zk = row[p];
+      for (int k = p; k < q; ++k) {
+        const double2 cs = rot[k];
+        const double zk1 = row[k + 1];
+        row[k] = cs.x * zk + cs.y * zk1;
+        zk = -cs.y * zk + cs.x * zk1;
+      }
+      row[q] = zk;
+    }
+    __syncwarp();
+  }
 }
 
-// Per-trajectory controller: eigen-solves, step search, coefficient rows.
+// One warp: c = exp(-i T_hi t) e1 (into `c` when non-null) and the embedded
+// error safety * norm * |c_hi(t) - [c_lo(t); 0]| (0 when `exact`), the
+// reference's estimate (rpm_statevector_engine.py:690-715).  ph: 2 * kBMaxK
+// warp-private scratch.  Records follow the krylov.cuh layout (LD = kBMaxK).
+__device__ double warp_step_error(const double* rec_hi, const double* rec_lo, bool exact, double t, double safety,
+                                  double norm, double2* ph, double2* c) {
+  const int lane = threadIdx.x & 31;
+  const int mh = (int)rec_hi[0], ml = exact ? 0 : (int)rec_lo[0];
+  const double* lh = rec_hi + 2;
+  const double* zh = rec_hi + 2 + kBMaxK;
+  const double* ll = rec_lo + 2;
+  const double* zl = rec_lo + 2 + kBMaxK;
+  for (int k = lane; k < mh + ml; k += 32) {
+    const bool hi = k < mh;
+    const int kk = hi ? k : k - mh;
+    double sv, cv;
+    sincos((hi ? lh : ll)[kk] * t, &sv, &cv);
+    const double w = (hi ? zh : zl)[kk];
+    ph[k] = make_double2(cv * w, -sv * w);
+  }
+  __syncwarp();
+  double acc = 0.0;
+  for (int i = lane; i < mh; i += 32) {
+    double2 ch = make_double2(0.0, 0.0), cl = make_double2(0.0, 0.0);
+    for (int k = 0; k < mh; ++k) {
+      const double zz = zh[i * kBMaxK + k];
+      ch.x = fma(zz, ph[k].x, ch.x);
+      ch.y = fma(zz, ph[k].y, ch.y);
+    }
+    if (c) c[i] = ch;
+    if (i < ml) {
+      for (int k = 0; k < ml; ++k) {
+        const double zz = zl[i * kBMaxK + k];
+        cl.x = fma(zz, ph[mh + k].x, cl.x);
+        cl.y = fma(zz, ph[mh + k].y, cl.y);
+      }
+    }
+    const double dx = ch.x - cl.x, dy = ch.y - cl.y;
+    acc = fma(dx, dx, fma(dy, dy, acc));
+  }
+  acc = warp_sum(acc);
+  __syncwarp();
+  return exact ? 0.0 : safety * norm * sqrt(acc);
+}
+
+// Per trajectory: spectra of T_M and T_{M-offset} (one warp each), the
+// largest step dt <= dt_max with err(dt) <= budget * dt / T (bracket, then
+// 5-way multisection in log dt with four trial steps per round, one per
+// warp, to a relative width of 5e-4), and the coefficient rows of the
+// step's observation points (one point per warp at a time).
 // Dynamic shared memory: two spectra records (hi, lo) of the krylov.cuh layout.
 __global__ void __launch_bounds__(128) k_b_control(BatchDev B) {
   extern __shared__ double sm[];
-  __shared__ double2 ph[kBMaxK], c[kBMaxK], clo[kBMaxK], rot[kBMaxK];
-  __shared__ double d[kBMaxK], e[kBMaxK], red[32];
-  __shared__ double s_dt;
-  __shared__ int s_ok;
+  __shared__ double2 ph[4][2 * kBMaxK];
+  __shared__ double2 rot[2][kBMaxK];
+  __shared__ double dd[2][kBMaxK], ee[2][kBMaxK];
+  __shared__ double cand[4];
+  __shared__ int okf[4];
+  __shared__ double s_dt, s_lo, s_hi;
+  __shared__ int s_state, s_np;
   const int b = blockIdx.x;
   TrajState& s = B.st[b];
   if (s.done) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double* rec_hi = sm;
   double* rec_lo = sm + kRecDoubles;
   const int M = s.msize;
   const bool exact = s.stop != 0;
   const int ML = max(1, M - B.offset);
-  // spectra of T_M and T_ML, written in the krylov.cuh record layout
-  for (int pass = 0; pass < (exact ? 1 : 2); ++pass) {
-    const int dim = pass == 0 ? M : ML;
-    double* rec = pass == 0 ? rec_hi : rec_lo;
-    for (int i = threadIdx.x; i < dim; i += blockDim.x) {
-      d[i] = s.alpha[i];
-      e[i] = (i + 1 < dim) ? s.beta[i] : 0.0;
+  if (warp < (exact ? 1 : 2)) {
+    const int dim = warp == 0 ? M : ML;
+    double* rec = warp == 0 ? rec_hi : rec_lo;
+    for (int i = lane; i < dim; i += 32) {
+      dd[warp][i] = s.alpha[i];
+      ee[warp][i] = (i + 1 < dim) ? s.beta[i] : 0.0;
     }
-    __syncthreads();
-    double* z = rec + 2 + kBMaxK;
-    const int bad = tridiag_qr(dim, d, e, z, kBMaxK, rot);
-    for (int i = threadIdx.x; i < dim; i += blockDim.x) rec[2 + i] = d[i];
-    if (threadIdx.x == 0) {
+    __syncwarp();
+    const int bad = tridiag_qr_warp(dim, dd[warp], ee[warp], rec + 2 + kBMaxK, kBMaxK, rot[warp]);
+    for (int i = lane; i < dim; i += 32) rec[2 + i] = dd[warp][i];
+    if (lane == 0) {
       rec[0] = dim;
       rec[1] = bad;
       if (bad) s.status = 2;
     }
-    __syncthreads();
   }
+  __syncthreads();
   const double t_now = s.t_now;
   const double remaining = B.t_end - t_now;
   double dt_max = fmin(B.max_step, remaining);
   // keep the observation points of one step within the coefficient buffer
   if (s.cursor + kMaxPts - 1 < B.ntimes) dt_max = fmin(dt_max, B.times[s.cursor + kMaxPts - 1] - t_now);
   const double norm = s.norm;
-  auto ok = [&](double dt) {
-    const double err = step_error(rec_hi, rec_lo, exact, dt, B.safety, norm, ph, c, clo, red);
-    return err <= B.budget * dt / B.t_end;
-  };
-  if (ok(dt_max)) {
-    if (threadIdx.x == 0) s_dt = dt_max;
-  } else {
-    // bracket [lo, hi] with ok(lo) and !ok(hi), then bisect in log scale
-    double hi = dt_max;
-    double lo = fmin(s.hint, 0.5 * dt_max);
-    int guard = 0;
-    while (!ok(lo) && guard < 60) {
-      hi = lo;
-      lo *= 0.25;
-      ++guard;
-    }
-    if (guard >= 60 || lo < B.min_step) {
-      if (threadIdx.x == 0) {
-        s.status = 3;  // step underflow
-        s.done = 1;
-        s.skip = 1;
-        atomicSub(B.active, 1);
-      }
-      return;
-    }
-    for (int it = 0; it < 24 && hi > lo * 1.0005; ++it) {
-      const double mid = sqrt(lo * hi);
-      if (ok(mid)) lo = mid;
-      else hi = mid;
-    }
-    if (threadIdx.x == 0) s_dt = lo;
+  if (threadIdx.x == 0) {
+    const double g = fmin(s.hint, 0.5 * dt_max);
+    cand[0] = dt_max;
+    cand[1] = g;
+    cand[2] = 0.25 * g;
+    cand[3] = 0.0625 * g;
+    s_state = 0;  // 0: first round, 1: going down, 2: multisection, 3: done, 4: underflow
+    s_lo = 0.0;
+    s_hi = dt_max;
   }
   __syncthreads();
+  for (int round = 0; round < 64; ++round) {
+    {
+      const double err = warp_step_error(rec_hi, rec_lo, exact, cand[warp], B.safety, norm, ph[warp], nullptr);
+      if (lane == 0) okf[warp] = err <= B.budget * cand[warp] / B.t_end;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int st = s_state;
+      if (st == 0 && okf[0]) {
+        s_dt = dt_max;
+        st = 3;
+      } else if (st == 0 || st == 1) {
+        int k0 = st == 0 ? 1 : 0, found = -1;
+        for (int k = k0; k < 4; ++k)
+          if (okf[k]) {
+            found = k;
+            break;
+          }
+        if (found >= 0) {
+          s_lo = cand[found];
+          s_hi = found == k0 ? s_hi : cand[found - 1];
+          if (found == k0 && st == 0) s_hi = dt_max;
+          st = 2;
+        } else {
+          s_hi = cand[3];
+          const double base = cand[3];
+          if (base * 0.25 < B.min_step) {
+            st = 4;
+          } else {
+            for (int k = 0; k < 4; ++k) cand[k] = base * pow(0.25, k + 1);
+            st = 1;
+          }
+        }
+      } else if (st == 2) {
+        for (int k = 0; k < 4; ++k) {
+          if (okf[k]) s_lo = cand[k];
+          else {
+            s_hi = cand[k];
+            break;
+          }
+        }
+      }
+      if (st == 2) {
+        if (s_lo < B.min_step) {
+          st = 4;
+        } else if (s_hi <= s_lo * 1.0005) {
+          s_dt = s_lo;
+          st = 3;
+        } else {
+          const double l0 = log(s_lo), w = log(s_hi) - l0;
+          for (int k = 0; k < 4; ++k) cand[k] = exp(l0 + w * (k + 1) / 5.0);
+        }
+      }
+      s_state = st;
+    }
+    __syncthreads();
+    if (s_state >= 3) break;
+  }
+  if (s_state != 3) {
+    if (threadIdx.x == 0) {
+      s.status = 3;  // step underflow (or no bracket within the round limit)
+      s.done = 1;
+      s.skip = 1;
+      atomicSub(B.active, 1);
+    }
+    return;
+  }
   double dt = s_dt;
   if (remaining - dt < 1e-12) dt = remaining;
-  // endpoint coefficients and error
-  const double err_end = step_error(rec_hi, rec_lo, exact, dt, B.safety, norm, ph, c, clo, red);
   double2* rows = B.coef + (size_t)b * (kMaxPts + 1) * kBMaxK;
-  for (int i = threadIdx.x; i < kBMaxK; i += blockDim.x) rows[(size_t)kMaxPts * kBMaxK + i] = i < M ? c[i] : make_double2(0, 0);
   // observation points inside (t_now, t_now + dt]
-  int np = 0;
-  const double t_end_step = t_now + dt;
-  while (s.cursor + np < B.ntimes && np < kMaxPts && B.times[s.cursor + np] <= t_end_step + 1e-13) {
-    const double tau = B.times[s.cursor + np] - t_now;
-    const double perr = step_error(rec_hi, rec_lo, exact, tau, B.safety, norm, ph, c, clo, red);
-    for (int i = threadIdx.x; i < kBMaxK; i += blockDim.x) rows[(size_t)np * kBMaxK + i] = i < M ? c[i] : make_double2(0, 0);
-    if (threadIdx.x == 0) B.perr[(size_t)b * kMaxPts + np] = perr;
-    ++np;
-  }
   if (threadIdx.x == 0) {
-    s.dt = dt;
-    s.step_err = err_end;
-    s.npts = np;
+    int np = 0;
+    const double t_end_step = t_now + dt;
+    while (s.cursor + np < B.ntimes && np < kMaxPts && B.times[s.cursor + np] <= t_end_step + 1e-13) ++np;
+    s_np = np;
+  }
+  __syncthreads();
+  const int np = s_np;
+  // point p < np: row p; p == np: the endpoint (row kMaxPts)
+  for (int p = warp; p <= np; p += 4) {
+    const bool endpoint = p == np;
+    const double tau = endpoint ? dt : B.times[s.cursor + p] - t_now;
+    double2* row = rows + (size_t)(endpoint ? kMaxPts : p) * kBMaxK;
+    const double err = warp_step_error(rec_hi, rec_lo, exact, tau, B.safety, norm, ph[warp], row);
+    for (int i = M + lane; i < kBMaxK; i += 32) row[i] = make_double2(0.0, 0.0);
+    if (lane == 0) {
+      if (endpoint) {
+        s.dt = dt;
+        s.step_err = err;
+        s.npts = np;
+      } else {
+        B.perr[(size_t)b * kMaxPts + p] = err;
+      }
+    }
   }
 }
 
@@ -591,6 +755,10 @@ struct rpm_batch {
   // on entry and before it on exit through events.
   cudaStream_t work = nullptr;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  // The singlet Gram depends only on the basis: it runs on `side`, forked
+  // from and joined back into `work`, concurrently with the controller.
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // Measurement: a timed event pair around the H psi of Lanczos iteration 1 of
   // every Krylov step (recorded inside the graph), sampled at each poll while
   // every trajectory is still running; and the number of kernels launched.
@@ -705,9 +873,13 @@ static void record_step(rpm_batch* Bh, const BatchDev& B, const Layout& L, cudaS
   Bh->fused = fused;
   Bh->launches_per_step = 1 + (fused ? 2 : 3) * m + 4;
   const size_t ctl_smem = sizeof(double) * 2 * kRecDoubles;
+  check_cuda(cudaEventRecord(Bh->ev_fork, st), "fork record");
+  check_cuda(cudaStreamWaitEvent(Bh->side, Bh->ev_fork, 0), "fork wait");
+  k_b_gram<<<dim3(B.gblk, B.ntraj), 256, 0, Bh->side>>>(B);
+  check_cuda(cudaEventRecord(Bh->ev_join, Bh->side), "join record");
   k_b_control<<<B.ntraj, 128, ctl_smem, st>>>(B);
   k_b_rebuild<<<ew, kEwThreads, 0, st>>>(B);
-  k_b_gram<<<dim3(B.gblk, B.ntraj), 256, 0, st>>>(B);
+  check_cuda(cudaStreamWaitEvent(st, Bh->ev_join, 0), "join wait");
   k_b_observe<<<B.ntraj, 256, sizeof(double2) * kBMaxK * kBMaxK, st>>>(B);
   check_launch("batched step");
 }
@@ -872,6 +1044,9 @@ int rpm_batch_create(rpm_system* const* systems, int nsys, const rpm_batch_confi
     check_cuda(cudaStreamCreateWithFlags(&B->work, cudaStreamNonBlocking), "create batch stream");
     check_cuda(cudaEventCreateWithFlags(&B->ev_in, cudaEventDisableTiming), "create event");
     check_cuda(cudaEventCreateWithFlags(&B->ev_out, cudaEventDisableTiming), "create event");
+    check_cuda(cudaStreamCreateWithFlags(&B->side, cudaStreamNonBlocking), "create batch stream");
+    check_cuda(cudaEventCreateWithFlags(&B->ev_fork, cudaEventDisableTiming), "create event");
+    check_cuda(cudaEventCreateWithFlags(&B->ev_join, cudaEventDisableTiming), "create event");
     check_cuda(cudaEventCreate(&B->probe0), "create probe event");
     check_cuda(cudaEventCreate(&B->probe1), "create probe event");
     check_cuda(cudaMalloc(&B->views_dev, sizeof(CubeView<float2>) * nsys), "cudaMalloc(views)");
@@ -919,8 +1094,12 @@ int rpm_batch_destroy(rpm_batch* batch) {
     if (!batch) return;
     free_graph(batch);
     if (batch->work) cudaStreamSynchronize(batch->work);
+    if (batch->side) cudaStreamSynchronize(batch->side);
     if (batch->buf) cudaFree(batch->buf);
     if (batch->views_dev) cudaFree(batch->views_dev);
+    if (batch->ev_fork) cudaEventDestroy(batch->ev_fork);
+    if (batch->ev_join) cudaEventDestroy(batch->ev_join);
+    if (batch->side) cudaStreamDestroy(batch->side);
     if (batch->ev_in) cudaEventDestroy(batch->ev_in);
     if (batch->ev_out) cudaEventDestroy(batch->ev_out);
     if (batch->probe0) cudaEventDestroy(batch->probe0);

@@ -53,10 +53,20 @@ def test_batched_path_reproduces_all_archived_yields():
     dims = hams[0].dimensions
     init = rb.random_phase_initial_state(dims, 20260731, 0)
     times = time_grid_us(HORIZON)
-    # a budget 100x tighter than the archived runs', so that the comparison is
-    # limited by the archived yields' own error estimate
+    # A budget 100x tighter than the archived runs'.  Over this 57.56-us
+    # horizon (about ten times the 5-us benchmark horizon) the complex64
+    # H psi has an accuracy floor of about 1e-6 in the yield: the FP32
+    # rounding of the Hamiltonian's coefficients is a fixed relative
+    # perturbation of H (~6e-8) whose phase error grows with time.  A
+    # tight-budget FP64 run of the last row agrees with its archived yield to
+    # 3e-12, so the archived yields are the reference and the bar is their
+    # own estimate plus that floor.
+    FP32_FLOOR = 1.5e-6
     bp = BatchedPropagator(hams, krylov_dimension=32, state_error_budget=2.4e-7)
     out = bp.propagate([init] * len(ROWS), times, system_index=list(range(len(ROWS))), lifetime_us=TAU)
+    errs = []
     for r, y in zip(ROWS, out.yields):
-        tol = float(r["yield_propagation_estimate"]) + float(r["quadrature_error"]) + 1e-7
-        assert abs(y - float(r["yield"])) < tol, (r, y)
+        tol = float(r["yield_propagation_estimate"]) + float(r["quadrature_error"]) + FP32_FLOOR
+        errs.append(abs(y - float(r["yield"])))
+        assert errs[-1] < tol, (r, y)
+    assert float(np.sqrt(np.mean(np.square(errs)))) < 1e-6
