@@ -39,6 +39,7 @@ UNIT = "trajectories/s"
 HORIZON_US = 5.0
 GRID_US = 0.00125
 LIFETIME_US = 1.0
+YIELD_TOL = 1e-6  # singlet-yield error bar of the metric
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -278,7 +279,21 @@ def b200_arm(args, rank: int, world: int, dist) -> None:
     states = np.stack([vecs[v] for k in range(args.orientations) for v in range(nvec)])
     system_index = np.array([k for k in range(args.orientations) for _ in range(nvec)], dtype=np.int32)
     times = np.arange(int(round(args.horizon / GRID_US)) + 1) * GRID_US
-    bp = BatchedPropagator(hams, krylov_dimension=args.krylov, state_error_budget=args.budget)
+    tuning = None
+    krylov, budget = args.krylov, args.budget
+    if krylov == "auto" or budget is None:
+        # Krylov dimension over the batched configuration's range 16-40 (tile
+        # fixed at this workload's batch), budget from the yield tolerance
+        from rpm_b200.autotune import KRYLOV_RANGE, budget_for_yield_tolerance, tune
+
+        if krylov == "auto":
+            tuning = tune(hams, list(states), system_index, horizon_us=0.25, yield_tolerance=YIELD_TOL,
+                          krylov_dimensions=KRYLOV_RANGE, tiles=(ntraj,))
+            krylov = tuning.krylov_dimension
+        if budget is None:
+            budget = budget_for_yield_tolerance(YIELD_TOL)
+    krylov = int(krylov)
+    bp = BatchedPropagator(hams, krylov_dimension=krylov, state_error_budget=budget)
     ld = bp.leading_dimension
     pristine = torch.zeros((ntraj, ld), dtype=torch.complex128, device=dev)
     pristine[:, :n].copy_(torch.from_numpy(states))
@@ -389,9 +404,13 @@ def b200_arm(args, rank: int, world: int, dist) -> None:
                                    f"pair (2 e + 11 spin-1/2 + 3 spin-1), {args.orientations} Fibonacci field "
                                    f"orientations x {nvec} random-phase vectors per GPU per step, {args.horizon:g} us, "
                                    f"0.00125-us grid ({len(times)} points), singlet yield tau = 1 us",
-                       "trajectories_per_step_per_gpu": ntraj, "krylov_dim": args.krylov,
-                       "state_error_budget": args.budget, "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (Krylov basis " f"{ntraj * (args.krylov + 1) * n * 8 / 1e9:.1f} GB)"},
+                       "trajectories_per_step_per_gpu": ntraj, "krylov_dim": krylov,
+                       "krylov_choice": ("autotuned over " + str([t["krylov_dimension"] for t in tuning.trials])
+                                         if tuning else "fixed"),
+                       "state_error_budget": budget, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (Krylov basis " f"{ntraj * (krylov + 1) * n * 8 / 1e9:.1f} GB)"},
+            "autotune": ({"trials": [{k: t[k] for k in ("krylov_dimension", "throughput") if k in t}
+                                     for t in tuning.trials], "horizon_us": 0.25} if tuning else None),
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -415,8 +434,9 @@ def main() -> None:
     p.add_argument("--impl", choices=("b200", "reference"), default="b200")
     p.add_argument("--orientations", type=int, default=12)
     p.add_argument("--vectors", type=int, default=4, help="random-phase vectors per orientation per GPU")
-    p.add_argument("--krylov", type=int, default=32)
-    p.add_argument("--budget", type=float, default=1e-7)
+    p.add_argument("--krylov", default="auto", help="Krylov dimension, or 'auto' (autotuned over 16-40)")
+    p.add_argument("--budget", type=float, default=None,
+                   help="accumulated state-error budget (default: half the 1e-6 yield tolerance)")
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--cpu-horizon", type=float, default=0.025, help="us of the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")

@@ -236,19 +236,24 @@ __device__ __forceinline__ void outer_coefs(const float2* tab, int k, int m, int
 }
 
 // ---------------------------------------------------------------------------
-// Pass R: 32 rows (eA, l) x all (eB, r) per CTA; lane = row.
+// Pass R: 16 rows (eA, l) x all (eB, r) per CTA; lane bits 0-3 = row, lane
+// bit 4 selects one of two outer indices of the warp's task.
 // ---------------------------------------------------------------------------
 template <int N1, int NH>
 struct PassR {
   using S = Shape<N1, NH>;
+  static constexpr int TR = 16;          // rows per CTA
   static constexpr int HR = S::HALF;
   static constexpr int NO = HR / 4;      // outer indices per row
+  static constexpr int NTASK = (NO + 1) / 2;  // warp tasks: two outer indices each
   static constexpr int RS = 2 * HR + 2;  // padded row stride (elements): an odd number of 16-byte units
   static constexpr int TAB_BYTES = align16c(S::NTAB * 8);
   static constexpr int OREC_BYTES = align16c(NO * (int)sizeof(ORec));
-  static constexpr int SMEM = TAB_BYTES + OREC_BYTES + 32 * RS * 8;
+  // tables, records, the tile and (fused Lanczos) the tile of v_{j-1}
+  static constexpr int SMEM = TAB_BYTES + OREC_BYTES + 2 * TR * RS * 8;
   // 8 warps: measured faster than 12 or 16, which force register spills
-  static constexpr int WARPS = NO % 8 == 0 ? 8 : NO % 6 == 0 ? 6 : NO % 4 == 0 ? 4 : NO % 3 == 0 ? 3 : NO < 8 ? NO : 8;
+  static constexpr int WARPS =
+      NTASK % 8 == 0 ? 8 : NTASK % 6 == 0 ? 6 : NTASK % 4 == 0 ? 4 : NTASK % 3 == 0 ? 3 : NTASK < 8 ? NTASK : 8;
   static_assert(NH >= 2, "pass R needs two trailing spin-1/2 digits");
 };
 
@@ -258,7 +263,7 @@ __global__ void __launch_bounds__(PassR<N1, NH>::WARPS * 32, 2)
   using P = PassR<N1, NH>;
   using S = typename P::S;
   constexpr int K = S::K;
-  constexpr int HR = P::HR, NO = P::NO, RS = P::RS;
+  constexpr int TR = P::TR, HR = P::HR, NO = P::NO, RS = P::RS;
   constexpr int NT = P::WARPS * 32;
   const int b = blockIdx.y;
   if (skip_vec(a, b)) return;
@@ -267,9 +272,10 @@ __global__ void __launch_bounds__(PassR<N1, NH>::WARPS * 32, 2)
   float2* tab = reinterpret_cast<float2*>(smem_raw);
   ORec* orec = reinterpret_cast<ORec*>(smem_raw + P::TAB_BYTES);
   float2* tile = reinterpret_cast<float2*>(smem_raw + P::TAB_BYTES + P::OREC_BYTES);
+  float2* ptile = tile + TR * RS;
   const int half_l = view->half_l;
-  const int row0 = blockIdx.x * 32;
-  const int rows = min(32, 2 * half_l - row0);
+  const int row0 = blockIdx.x * TR;
+  const int rows = min(TR, 2 * half_l - row0);
   const long long quarter = (long long)half_l * HR;
   const float2* x_in = a.in + (long long)b * a.ld;
   constexpr int CH = HR / 2;  // 16-byte chunks per half row
@@ -283,50 +289,16 @@ __global__ void __launch_bounds__(PassR<N1, NH>::WARPS * 32, 2)
     slot = rr * RS + e * HR + 2 * c;
     g = (2 * ea + e) * quarter + (long long)llo * HR + 2 * c;
   };
-  if (a.lz.on && !a.lz.first) {
-    // v_j = (w'_j - alpha_{j-1} v_{j-1}) * scale, staged and written back into `in`
-    const float al = (float)a.lz.alpha_prev[(long long)b * a.lz.dstride];
-    const float sc = (float)in_scale(a, b);
-    const float2* pv = a.lz.prev + (long long)b * a.ld;
-    float2* xo = const_cast<float2*>(x_in);
-    constexpr int UB = 6;  // units per thread in flight
-    for (int base = threadIdx.x; base < units; base += NT * UB) {
-      float4 w[UB], q[UB];
-#pragma unroll
-      for (int u = 0; u < UB; ++u) {
-        const int idx = base + u * NT;
-        if (idx < units) {
-          int slot;
-          long long g;
-          unit_at(idx, slot, g);
-          w[u] = __ldcg(reinterpret_cast<const float4*>(x_in + g));
-          q[u] = __ldcg(reinterpret_cast<const float4*>(pv + g));
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < UB; ++u) {
-        const int idx = base + u * NT;
-        if (idx < units) {
-          int slot;
-          long long g;
-          unit_at(idx, slot, g);
-          float4 v;
-          v.x = sc * fmaf(-al, q[u].x, w[u].x);
-          v.y = sc * fmaf(-al, q[u].y, w[u].y);
-          v.z = sc * fmaf(-al, q[u].z, w[u].z);
-          v.w = sc * fmaf(-al, q[u].w, w[u].w);
-          *reinterpret_cast<float4*>(tile + slot) = v;
-          *reinterpret_cast<float4*>(xo + g) = v;
-        }
-      }
-    }
-  } else {
-    for (int idx = threadIdx.x; idx < units; idx += NT) {
-      int slot;
-      long long g;
-      unit_at(idx, slot, g);
-      copy16(tile + slot, x_in + g);
-    }
+  // fused Lanczos (j > 0): the tile receives w'_j and ptile v_{j-1}; below,
+  // v_j = (w'_j - alpha_{j-1} v_{j-1}) * scale replaces w'_j in the tile and in `in`
+  const bool combine = a.lz.on && !a.lz.first;
+  const float2* pv = combine ? a.lz.prev + (long long)b * a.ld : nullptr;
+  for (int idx = threadIdx.x; idx < units; idx += NT) {
+    int slot;
+    long long g;
+    unit_at(idx, slot, g);
+    copy16(tile + slot, x_in + g);
+    if (combine) copy16(ptile + slot, pv + g);
   }
   for (int k = threadIdx.x; k < S::NTAB; k += NT) tab[k] = view->tabR[k];
   __syncthreads();
@@ -348,19 +320,42 @@ __global__ void __launch_bounds__(PassR<N1, NH>::WARPS * 32, 2)
     orec[o] = r;
   }
   copy_wait_all();
+  if (combine) {
+    // each thread combines the units it copied (visible to it after its own wait)
+    const float al = (float)a.lz.alpha_prev[(long long)b * a.lz.dstride];
+    const float sc = (float)in_scale(a, b);
+    float2* xo = const_cast<float2*>(x_in);
+    for (int idx = threadIdx.x; idx < units; idx += NT) {
+      int slot;
+      long long g;
+      unit_at(idx, slot, g);
+      const float4 w = *reinterpret_cast<const float4*>(tile + slot);
+      const float4 q = *reinterpret_cast<const float4*>(ptile + slot);
+      float4 v;
+      v.x = sc * fmaf(-al, q.x, w.x);
+      v.y = sc * fmaf(-al, q.y, w.y);
+      v.z = sc * fmaf(-al, q.z, w.z);
+      v.w = sc * fmaf(-al, q.w, w.w);
+      *reinterpret_cast<float4*>(tile + slot) = v;
+      *reinterpret_cast<float4*>(xo + g) = v;
+    }
+  }
   __syncthreads();
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int row = lane & 15, hsel = lane >> 4;
   const float sf = a.lz.on ? 1.0f : (float)in_scale(a, b);  // fused: the staged v_j is already scaled
-  const float2* rowp = tile + lane * RS;
+  const float2* rowp = tile + row * RS;
   float din[2][4];
   float2 fin[2][4];
   cube_consts<S>(tab, din, fin);
-  const int rho = row0 + lane;
+  const int rho = row0 + row;
   const int ea = rho >= half_l ? 1 : 0;
   const long long gbase = 2 * ea * quarter + (long long)(rho - ea * half_l) * HR;
   float2* y_b = yb + (long long)b * (a.ya_ld ? a.ya_ld : a.ld) + gbase;
-  for (int o = warp; o < NO; o += P::WARPS) {
+  for (int t = warp; t < P::NTASK; t += P::WARPS) {
+    const int o = min(2 * t + hsel, NO - 1);  // (odd NO: the spare half repeats the last index, no store)
+    const bool active = 2 * t + hsel < NO && row < rows;
     const ORec rec = orec[o];
     auto load = [&](int delta, float2 (&y)[2][4]) {
 #pragma unroll
@@ -387,15 +382,15 @@ __global__ void __launch_bounds__(PassR<N1, NH>::WARPS * 32, 2)
     for (int k = 0; k < K - 2; ++k) {
       const int m = (o / (S::gs(k) / 4)) % S::dim(k);
 #pragma unroll
-      for (int t = 1; t < S::dim(k); ++t) {
-        const int mp = m + t >= S::dim(k) ? m + t - S::dim(k) : m + t;
+      for (int tt = 1; tt < S::dim(k); ++tt) {
+        const int mp = m + tt >= S::dim(k) ? m + tt - S::dim(k) : m + tt;
         float2 c[2][2], y[2][4];
         outer_coefs<S>(tab, k, m, mp, c);
         load((mp - m) * S::gs(k), y);
         partner_mac(c, y, acc);
       }
     }
-    if (lane < rows) {
+    if (active) {
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const long long at = e * quarter + 4 * o;
@@ -617,7 +612,7 @@ void launch_r(const HpsiArgs<float2>& a, float2* yb, int half_l, int batch, cuda
   using P = PassR<N1, NH>;
   auto kern = fast_pass_r<N1, NH>;
   set_smem(kern, P::SMEM);
-  kern<<<dim3((2 * half_l + 31) / 32, batch), P::WARPS * 32, P::SMEM, st>>>(a, yb);
+  kern<<<dim3((2 * half_l + P::TR - 1) / P::TR, batch), P::WARPS * 32, P::SMEM, st>>>(a, yb);
   check_launch("fast_pass_r");
 }
 
