@@ -103,7 +103,7 @@ int rpm_system_fast_hpsi(const rpm_system* sys, int* usable);
  * (run loops of frameworks that own all device memory through a pool or
  * arena, fixed-budget embedded runtimes, code running while its owner
  * captures the stream into a CUDA graph).  Its only scratch, batch x ld
- * elements of the pass-L partial, lives in a 4 MiB array compiled into the
+ * elements of the partial result between the two radical passes, lives in a 4 MiB array compiled into the
  * library, which every GPU that loads the library keeps until process exit;
  * larger batch x ld x element-size requests fail with RPM_E_UNSUPPORTED.
  * The first call on each device looks up that array's device address (and

@@ -902,7 +902,7 @@ extern "C" int rpm_hpsi(rpm_system* sys, int precision, const void* psi_dev, voi
 // pool or arena they own), embedded runtimes with a fixed memory budget
 // decided at start-up, and code that runs while its owner is capturing a
 // stream into a CUDA graph.  rpm_hpsi grows a per-system cudaMalloc'd buffer
-// for the only scratch the radical-split action needs, the pass-L partial
+// for the only scratch the radical-split action needs, the partial result
 // (batch x ld elements).  This variant uses a fixed array compiled into the
 // library instead, so every GPU that loads the library holds those bytes
 // until the process exits.
