@@ -98,6 +98,32 @@ int rpm_set_cube_tuning(int ni_l, int ni_r, int tr, int tl);
  * a compiled digit pattern), else 0.  Diagnostic; no reference counterpart. */
 int rpm_system_fast_hpsi(const rpm_system* sys, int* usable);
 
+/* Reduced density matrices of a bipartition for `nstates` states spaced `ld`
+ * elements apart (complex128): rho[s][a][b] = sum_c psi_s[offa[a] + offc[c]]
+ * conj(psi_s[offa[b] + offc[c]]), a, b < da, c < dc; offa_dev/offc_dev are
+ * device int64 offset tables of the kept and traced axes.  Its eigenvalues
+ * are the squared Schmidt coefficients behind CORE:311-328
+ * (pure_log_negativity) and CORE:331-334 (reduced_electron_density). */
+int rpm_reduced_density(const void* states_dev, long long nstates, long long ld, const long long* offa_dev, int da,
+                        const long long* offc_dev, long long dc, void* rho_dev, void* stream);
+
+/* Squared Schmidt coefficients from the eigenvectors of rho_A (u_dev: per
+ * state da x da complex128, column i = eigenvector i):
+ * sigma2[s][i] = sum_c |sum_a conj(U[a][i]) psi_s[offa[a] + offc[c]]|^2,
+ * accurate for small Schmidt values, for CORE:311-328 (pure_log_negativity). */
+int rpm_schmidt_norms(const void* states_dev, long long nstates, long long ld, const long long* offa_dev, int da,
+                      const long long* offc_dev, long long dc, const void* u_dev, double* sigma2_dev, void* stream);
+
+/* Transition lines of one radical for the factorized ensemble yield
+ * (rpm_quantum_needle_reproduction.py:128-170): line (i, j) of the d
+ * eigenvalues lam_dev has frequency lam[i] - lam[j] and weight
+ * sp[i][j] sq[j][i] * scale (sp, sq: d x d complex128 electron-spin operators
+ * in the eigenbasis, row-major) and is deposited with linear interpolation
+ * onto grid_dev (2 * half_width + 1 complex128 bins of width delta, centred);
+ * a line outside the grid sets *bad_dev = 1. */
+int rpm_bin_transition_lines(const double* lam_dev, const void* sp_dev, const void* sq_dev, int d, double scale,
+                             double delta, long long half_width, void* grid_dev, int* bad_dev, void* stream);
+
 /* rpm_hpsi without any device allocation.  It has no counterpart in the
  * reference.  It serves callers that may not call cudaMalloc while they run
  * (run loops of frameworks that own all device memory through a pool or

@@ -758,3 +758,43 @@ def propagate_segments(initial_state, times_us, segments, *, state_error_budget=
         if pulse is not None and boundary < times[-1] - 1e-12:
             state = local_unitary_apply(state, dims, pulse[0], pulse[1])
     return values, bounds, state, tuple(counts), acc
+
+
+# ---------------------------------------------------------------------------
+# Entanglement observables of stored states (CORE:311-365)
+# ---------------------------------------------------------------------------
+def schmidt_values(state, dimensions: Sequence[int], left_axes: Sequence[int]) -> np.ndarray:
+    """Singular values of the state reshaped left axes x rest (CORE:317-323)."""
+    dims = tuple(int(v) for v in dimensions)
+    left = tuple(int(v) for v in left_axes)
+    right = tuple(a for a in range(len(dims)) if a not in left)
+    tensor = np.asarray(state, dtype=complex).reshape(dims)
+    matrix = np.transpose(tensor, left + right).reshape(math.prod(dims[a] for a in left), -1)
+    return np.linalg.svd(matrix, compute_uv=False)
+
+
+def pure_log_negativity(state, dimensions: Sequence[int], left_axes: Sequence[int]) -> float:
+    """2 log2 of the sum of normalised Schmidt values (CORE:311-328)."""
+    dims = tuple(int(v) for v in dimensions)
+    left = tuple(int(v) for v in left_axes)
+    if len(set(left)) != len(left) or any(a < 0 or a >= len(dims) for a in left):
+        raise ValueError("Invalid subsystem axes.")
+    sv = schmidt_values(state, dims, left)
+    norm = float(np.linalg.norm(sv))
+    if norm == 0.0:
+        raise ValueError("Cannot evaluate entanglement of the zero state.")
+    return float(2.0 * np.log2(np.sum(sv / norm)))
+
+
+def reduced_electron_density(state, dimensions: Sequence[int]) -> np.ndarray:
+    """Hermitised electron-pair density matrix, state reshaped 4 x rest (CORE:331-334)."""
+    m = np.asarray(state, dtype=complex).reshape(4, -1)
+    rho = m @ m.conj().T
+    return 0.5 * (rho + rho.conj().T)
+
+
+def mixed_two_electron_log_negativity(rho) -> float:
+    """max(0, log2 sum |eig(rho^T_A)|) of a hermitised 4 x 4 matrix (CORE:337-351)."""
+    h = 0.5 * (np.asarray(rho, dtype=complex) + np.asarray(rho, dtype=complex).conj().T)
+    pt = h.reshape(2, 2, 2, 2).transpose(2, 1, 0, 3).reshape(4, 4)
+    return float(max(0.0, np.log2(np.sum(np.abs(np.linalg.eigvalsh(pt))))))

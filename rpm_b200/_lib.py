@@ -85,6 +85,9 @@ SIGNATURES: dict[str, list] = {
     "rpm_hpsi_noalloc": [_P, _I, _P, _P, _I, _LL, _P],
     "rpm_set_cube_tuning": [_I, _I, _I, _I],
     "rpm_system_fast_hpsi": [_P, _PI],
+    "rpm_reduced_density": [_P, _LL, _LL, _P, _I, _P, _LL, _P, _P],
+    "rpm_bin_transition_lines": [_P, _P, _P, _I, _D, _D, _LL, _P, _P, _P],
+    "rpm_schmidt_norms": [_P, _LL, _LL, _P, _I, _P, _LL, _P, _P, _P],
     "rpm_apply_local_operator": [_PI, _I, _I, _PD, _P, _P, _I, _LL, _P],
     "rpm_lanczos_basis": [_P, _P, _I, _D, _P, _P, _P, _PI, _PD, _P],
     "rpm_tridiag_spectra": [_P, _P, _I, _PI, _P, _P],

@@ -120,8 +120,13 @@ def dimensions_for(nuclei: Sequence[Nucleus]) -> tuple[int, ...]:
     return (2, 2) + tuple(n.dimension for n in nuclei)
 
 
+ENTANGLEMENT_NUCLEAR_COUNTS = (4, 6, 8, 10, 12, 14)
+
+
 def selected_nuclei(nuclear_count: int) -> tuple[Nucleus, ...]:
     """Equal strongest-first prefixes of the two radicals (core.py:135-142)."""
+    if int(nuclear_count) not in ENTANGLEMENT_NUCLEAR_COUNTS:
+        raise ValueError(f"nuclear_count must be one of {ENTANGLEMENT_NUCLEAR_COUNTS}.")
     per = int(nuclear_count) // 2
     return tuple(FAD_NUCLEI[:per] + ALL_NUCLEI[len(FAD_NUCLEI):][:per])
 
@@ -195,6 +200,45 @@ def random_phase_initial_state(dimensions: Sequence[int], master_seed: int, samp
     out[m:2 * m] = nuclei / math.sqrt(2.0)
     out[2 * m:3 * m] = -nuclei / math.sqrt(2.0)
     return out
+
+
+def full_product_basis_indices(master_seed: int, sample_id: int) -> tuple[int, ...]:
+    """One reproducible computational product state of the 14 nuclei (core.py:261-265)."""
+    rng = np.random.default_rng(sample_seed(master_seed, sample_id))
+    return tuple(int(rng.integers(d)) for d in SYSTEM_DIMENSIONS[2:])
+
+
+def paired_product_indices(nuclear_count: int, full_indices: Sequence[int]) -> tuple[int, ...]:
+    """The FAD and TrpH prefixes of a 14-nucleus product state (core.py:280-282)."""
+    per = int(nuclear_count) // 2
+    return tuple(full_indices[:per]) + tuple(full_indices[7:7 + per])
+
+
+def product_basis_initial_state(dimensions: Sequence[int], indices: Sequence[int]) -> np.ndarray:
+    """Electron singlet x one nuclear computational basis state (core.py:268-277)."""
+    dims = tuple(int(v) for v in dimensions)
+    if len(indices) != len(dims) - 2:
+        raise ValueError("One product-basis index is required per nuclear axis.")
+    nuclei = np.zeros(math.prod(dims[2:]), dtype=complex)
+    nuclei[int(np.ravel_multi_index(tuple(int(i) for i in indices), dims[2:]))] = 1.0
+    singlet = np.array([0.0, 1.0, -1.0, 0.0], dtype=complex) / math.sqrt(2.0)
+    return np.kron(singlet, nuclei)
+
+
+def entanglement_time_grids_us() -> tuple[np.ndarray, np.ndarray]:
+    """Nested fine/coarse grids of the 0-2 us entanglement average (core.py:107-126).
+
+    Fine: 0-0.1 us every 0.000125 us, then every 0.0025 us to 2 us; coarse:
+    twice both spacings, an exact subset (its indices into the fine grid are
+    returned).
+    """
+    fine = np.concatenate((np.arange(0.0, 0.1 + 0.0000625, 0.000125), np.arange(0.1025, 2.0 + 0.00125, 0.0025)))
+    coarse = np.concatenate((np.arange(0.0, 0.1 + 0.000125, 0.00025), np.arange(0.105, 2.0 + 0.0025, 0.005)))
+    fine[-1] = coarse[-1] = 2.0
+    indices = np.searchsorted(fine, coarse)
+    if not np.allclose(fine[indices], coarse, rtol=0.0, atol=1e-13):
+        raise RuntimeError("Entanglement quadrature grids are not nested.")
+    return fine, indices
 
 
 def integrate_yield(times_us, populations, lifetime_us: float) -> float:
