@@ -180,3 +180,118 @@ class BatchedPropagator:
         if bad:
             raise RuntimeError(STATUS_TEXT.get(bad[0], f"batched propagation failed (status {bad[0]})"))
         return BatchedResult(times, vals, bounds, se, yields, psi if return_final_states else None, st, status)
+
+
+@dataclass(frozen=True)
+class BatchedSegment:
+    """One segment of a batched segment propagation: trajectory b evolves under
+    ``hamiltonians[system_index[b]]`` until ``end_us``; then ``pulse``
+    (``(axis, unitary)`` or None) is applied to every trajectory unless
+    ``end_us`` is the final time."""
+
+    end_us: float
+    hamiltonians: Sequence
+    system_index: Sequence[int]
+    pulse: tuple | None = None
+
+
+def propagate_segments_batched(initial_states, times_us, segments: Sequence[BatchedSegment], *,
+                               state_error_budget: float = 5e-7, lifetime_us: float | None = None,
+                               krylov_dimension: int = 32, **knobs) -> BatchedResult:
+    """Batched counterpart of :func:`rpm_b200.segments.propagate_segments`.
+
+    Mirrors the reference's pulsed-control loop
+    (``rpm_nuclear_spin_rotation_control.py:281-308``) for many trajectories at
+    once: the horizon is cut at the segment ends; each segment runs the batched
+    propagator with that segment's systems over the observation times inside
+    it (shifted to start at the segment's start) with the budget scaled by the
+    segment's duration; observation points carry the errors accumulated by
+    earlier segments; between segments an instantaneous d x d unitary acts on
+    one tensor axis of every state on the GPU.  A segment's systems may differ
+    per trajectory (e.g. a field pulse of a per-trajectory amplitude); all
+    segments must give each trajectory systems of the same dimensions.
+    """
+    torch = _torch()
+    times = np.asarray(times_us, dtype=float)
+    if times.ndim != 1 or times.size == 0 or times[0] != 0.0 or np.any(np.diff(times) <= 0.0):
+        raise ValueError("Observation times must start at 0 and be strictly increasing.")
+    segs = list(segments)
+    if not segs or abs(segs[-1].end_us - times[-1]) > 1e-12:
+        raise ValueError("The last segment must end at the final observation time.")
+    ends = [s.end_us for s in segs]
+    if any(b <= a for a, b in zip(ends, ends[1:])) or ends[0] <= 0.0:
+        raise ValueError("Segment end times must be positive and strictly increasing.")
+    ntraj = len(initial_states)
+    for s in segs:
+        if len(s.system_index) != ntraj:
+            raise ValueError("every segment needs one system index per trajectory")
+    def budget_of(k: int) -> float:
+        start = 0.0 if k == 0 else float(segs[k - 1].end_us)
+        return state_error_budget * (float(segs[k].end_us) - start) / times[-1]
+
+    first = BatchedPropagator(segs[0].hamiltonians, krylov_dimension=krylov_dimension,
+                              state_error_budget=budget_of(0), **knobs)
+    idx0 = np.asarray(segs[0].system_index, dtype=np.int32)
+    psi = first.load_states(initial_states, idx0)
+    ld = first.leading_dimension
+    dims = segs[0].hamiltonians[int(idx0[0])].dimensions
+    n = int(np.prod(dims))
+    values = np.empty((ntraj, times.size))
+    errors = np.empty((ntraj, times.size))
+    p0 = np.empty(ntraj)
+    _lib.call("rpm_singlet_population", _lib.ptr(psi), n, ntraj, ld, _lib.dptr(p0), _lib.stream_handle())
+    values[:, 0] = p0
+    errors[:, 0] = 0.0
+    accumulated = np.zeros(ntraj)
+    accepted = np.zeros(ntraj, dtype=np.int64)
+    matvecs = np.zeros(ntraj, dtype=np.int64)
+    min_step = np.full(ntraj, np.inf)
+    max_step = np.zeros(ntraj)
+    cursor, current = 1, 0.0
+    for k, seg in enumerate(segs):
+        boundary = float(seg.end_us)
+        stop = int(np.searchsorted(times, boundary + 1e-12, side="right"))
+        requested = times[cursor:stop] - current
+        duration = boundary - current
+        local = requested if requested.size and requested[-1] >= duration - 1e-12 else np.append(requested, duration)
+        idx = np.asarray(seg.system_index, dtype=np.int32)
+        bp = first if k == 0 else BatchedPropagator(seg.hamiltonians, krylov_dimension=krylov_dimension,
+                                                    state_error_budget=budget_of(k), **knobs)
+        if bp.leading_dimension != ld:
+            raise ValueError("all segments must use systems of the same dimensions")
+        vals, errs, stats = bp.propagate_device(psi, local, idx)
+        count = requested.size
+        v = vals[:, :count].cpu().numpy()
+        e = errs[:, :count].cpu().numpy()
+        values[:, cursor:stop] = v
+        errors[:, cursor:stop] = accumulated[:, None] + e
+        bad = [int(s.status) for s in stats if s.status]
+        if bad:
+            raise RuntimeError(STATUS_TEXT.get(bad[0], f"batched propagation failed (status {bad[0]})"))
+        accumulated += np.array([s.accumulated_state_error for s in stats])
+        accepted += np.array([s.accepted_steps for s in stats])
+        matvecs += np.array([s.matvecs for s in stats])
+        min_step = np.minimum(min_step, [s.minimum_step_us if s.accepted_steps else np.inf for s in stats])
+        max_step = np.maximum(max_step, [s.maximum_step_us for s in stats])
+        cursor, current = stop, boundary
+        if seg.pulse is not None and boundary < times[-1] - 1e-12:
+            axis, unitary = seg.pulse
+            op = np.ascontiguousarray(unitary, dtype=np.complex128)
+            dd = np.ascontiguousarray(dims, dtype=np.int32)
+            out = torch.empty_like(psi)
+            _lib.call("rpm_apply_local_operator", _lib.iptr(dd), len(dd), int(axis), op.ctypes.data_as(_lib._PD),
+                      _lib.ptr(psi), _lib.ptr(out), ntraj, ld, _lib.stream_handle())
+            psi = out
+    yields = None
+    if lifetime_us is not None:
+        vt = torch.from_numpy(np.ascontiguousarray(values)).to("cuda")
+        t = torch.as_tensor(times, device="cuda")
+        out = torch.empty(ntraj, dtype=torch.float64, device="cuda")
+        _lib.call("rpm_simpson_yield", _lib.ptr(t), _lib.ptr(vt), int(times.size), ntraj, int(times.size),
+                  float(lifetime_us), _lib.ptr(out), _lib.stream_handle())
+        yields = out.cpu().numpy()
+    bounds = np.vectorize(state_error_to_population_bound)(errors)
+    st = tuple(PropagationStats(int(accepted[b]), 0, int(matvecs[b]), int(krylov_dimension),
+                                float(min_step[b]) if np.isfinite(min_step[b]) else 0.0, float(max_step[b]),
+                                float(accumulated[b]), 0.0) for b in range(ntraj))
+    return BatchedResult(times, values, bounds, errors, yields, psi, st, np.zeros(ntraj, dtype=np.int32))

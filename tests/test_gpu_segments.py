@@ -71,3 +71,56 @@ def test_square_field_pulse_matches_oracle():
     assert (got.accepted_steps, got.rejected_steps, got.matvecs) == ref[3]
     y_got = oracle.integrate_yield(times, got.observable_values, 1.0)
     assert abs(y_got - oracle.integrate_yield(times, ref[0], 1.0)) < 1e-11
+
+
+def test_batched_square_pulse_matches_plain_segments():
+    """Config-3-style transverse square pulse with a per-trajectory amplitude, batched vs plain FP64."""
+    import rpm_b200 as rb
+    from rpm_b200 import segments, synthetic
+    from rpm_b200.batched import BatchedSegment, propagate_segments_batched
+
+    sysm = synthetic.prefix_system(synthetic.full_system(), 5)
+    theta, phi = 0.6, 0.0
+    amps_nT = (0.0, 250.0, 500.0)
+    transverse = np.array([math.cos(theta), 0.0, -math.sin(theta)])  # perpendicular to the static field in zx
+    h0 = rb.CompiledFullPairHamiltonian(sysm.dimensions, sysm.terms(theta, phi), left_axes=sysm.left_axes,
+                                        right_axes=sysm.right_axes)
+    hp = [rb.CompiledFullPairHamiltonian(sysm.dimensions, sysm.terms(theta, phi, extra_field_mT=a * 1e-6 * transverse),
+                                         left_axes=sysm.left_axes, right_axes=sysm.right_axes) for a in amps_nT]
+    assert h0._system.fast_hpsi
+    psi = synthetic.random_phase_vectors(sysm.dimensions, len(amps_nT), 21)
+    times = np.arange(321) * 0.00125  # 0 .. 0.4 us; pulse on [0.1, 0.25)
+    start, dur = 0.1, 0.15
+    nb = len(amps_nT)
+    segs = [BatchedSegment(start, [h0], [0] * nb), BatchedSegment(start + dur, hp, list(range(nb))),
+            BatchedSegment(times[-1], [h0], [0] * nb)]
+    out = propagate_segments_batched(list(psi), times, segs, state_error_budget=1e-8, lifetime_us=1.0,
+                                     krylov_dimension=32)
+    for b, a in enumerate(amps_nT):
+        ref = segments.propagate_segments(psi[b], times, segments.square_pulse_segments(h0, hp[b], start, dur, times[-1]),
+                                          state_error_budget=1e-10, **KNOBS)
+        assert np.max(np.abs(out.observable_values[b] - ref.observable_values)) < 1e-5
+        assert abs(out.yields[b] - rb.integrate_yield(times, ref.observable_values, 1.0)) < 1e-6
+    # the pulse changes the dynamics: trajectories differ only through it
+    assert np.max(np.abs(out.observable_values[2] - out.observable_values[0])) > 1e-4 or amps_nT[2] == 0.0
+
+
+def test_batched_periodic_pi_pulses_match_plain_segments():
+    import rpm_b200 as rb
+    from rpm_b200 import segments, synthetic
+    from rpm_b200.batched import BatchedSegment, propagate_segments_batched
+
+    sysm = synthetic.prefix_system(synthetic.full_system(), 5)
+    h = rb.CompiledFullPairHamiltonian(sysm.dimensions, sysm.terms(0.9, 0.3), left_axes=sysm.left_axes,
+                                       right_axes=sysm.right_axes)
+    psi = synthetic.random_phase_vectors(sysm.dimensions, 2, 8)
+    times = np.arange(241) * 0.00125
+    u = segments.spin_pi_pulse(1.0, [0.0, 0.2, 1.0])
+    ends = [0.05, 0.13, 0.21, 0.3]
+    out = propagate_segments_batched(list(psi), times, [BatchedSegment(e, [h], [0, 0], (2, u)) for e in ends],
+                                     state_error_budget=1e-8, lifetime_us=1.0)
+    for b in range(2):
+        ref = segments.propagate_segments(psi[b], times, [segments.Segment(e, h, (2, u)) for e in ends],
+                                          state_error_budget=1e-10, **KNOBS)
+        assert np.max(np.abs(out.observable_values[b] - ref.observable_values)) < 1e-5
+        assert abs(out.yields[b] - rb.integrate_yield(times, ref.observable_values, 1.0)) < 1e-6
