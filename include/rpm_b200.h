@@ -92,6 +92,18 @@ int rpm_hpsi(rpm_system* sys, int precision, const void* psi_dev, void* out_dev,
  * back to the heuristic.  Used by the autotuner; no reference counterpart. */
 int rpm_set_cube_tuning(int ni_l, int ni_r, int tr, int tl);
 
+/* Haberkorn recombination with singlet / triplet rates (1/us) on a radical-
+ * split system, for the batched propagator: the state evolves under
+ * H - (i/2)(kS P_S + kT P_T); the common decay exp(-min(kS, kT) t / 2) is
+ * factored out and the remaining -(i/2)|kS - kT| Q (Q = P_S or P_T, an
+ * electron-pair operator) is added to the pair operator.  Unequal rates make
+ * the system non-Hermitian: the plain Lanczos path refuses it and the batched
+ * path runs Arnoldi.  Set the rates before creating a batch from the system.
+ * The reference has equal rates only (its yield weight exp(-t/tau)/tau);
+ * unequal rates have no reference counterpart. */
+int rpm_system_set_recombination(rpm_system* sys, double singlet_rate, double triplet_rate);
+int rpm_system_recombination(const rpm_system* sys, double* singlet_rate, double* triplet_rate, int* non_hermitian);
+
 /* *usable = 1 when complex64 H psi of this system runs on the shape-
  * specialised kernels (axes ordered electron A, electron B, left nuclei,
  * right nuclei; each radical's spin-1 nuclei before its spin-1/2 nuclei;

@@ -798,3 +798,35 @@ def mixed_two_electron_log_negativity(rho) -> float:
     h = 0.5 * (np.asarray(rho, dtype=complex) + np.asarray(rho, dtype=complex).conj().T)
     pt = h.reshape(2, 2, 2, 2).transpose(2, 1, 0, 3).reshape(4, 4)
     return float(max(0.0, np.log2(np.sum(np.abs(np.linalg.eigvalsh(pt))))))
+
+
+# ---------------------------------------------------------------------------
+# Unequal Haberkorn rates (no reference implementation: dense restatement)
+# ---------------------------------------------------------------------------
+def haberkorn_dense(h_dense, dimensions: Sequence[int], psi0, times_us, singlet_rate: float, triplet_rate: float):
+    """Singlet populations and yield under H - (i/2)(kS P_S + kT P_T), dense.
+
+    The state is propagated exactly (eigen-decomposition of the non-Hermitian
+    dense operator).  Returns (populations of the state with the common decay
+    exp(-min(kS, kT) t / 2) factored out, singlet yield kS int P_S(t) dt on the
+    grid by Simpson's rule).  Electrons are axes 0, 1 (C order, slowest).
+    """
+    dims = tuple(int(v) for v in dimensions)
+    n = math.prod(dims)
+    m = n // 4
+    ps4 = np.zeros((4, 4), dtype=complex)
+    ps4[1, 1] = ps4[2, 2] = 0.5
+    ps4[1, 2] = ps4[2, 1] = -0.5
+    ps = np.kron(ps4, np.eye(m))
+    heff = np.asarray(h_dense, dtype=complex) - 0.5j * (singlet_rate * ps + triplet_rate * (np.eye(n) - ps))
+    w, v = np.linalg.eig(heff)
+    coeff = np.linalg.solve(v, np.asarray(psi0, dtype=complex))
+    times = np.asarray(times_us, dtype=float)
+    pops = np.empty(times.size)
+    for k, t in enumerate(times):
+        psi = v @ (np.exp(-1j * w * t) * coeff)
+        pops[k] = singlet_population(psi, dims)
+    kmin = min(singlet_rate, triplet_rate)
+    factored = pops * np.exp(kmin * times)
+    yield_value = singlet_rate * simpson(pops, times)
+    return factored, yield_value

@@ -88,6 +88,8 @@ SIGNATURES: dict[str, list] = {
     "rpm_reduced_density": [_P, _LL, _LL, _P, _I, _P, _LL, _P, _P],
     "rpm_bin_transition_lines": [_P, _P, _P, _I, _D, _D, _LL, _P, _P, _P],
     "rpm_schmidt_norms": [_P, _LL, _LL, _P, _I, _P, _LL, _P, _P, _P],
+    "rpm_system_set_recombination": [_P, _D, _D],
+    "rpm_system_recombination": [_P, _PD, _PD, _PI],
     "rpm_apply_local_operator": [_PI, _I, _I, _PD, _P, _P, _I, _LL, _P],
     "rpm_lanczos_basis": [_P, _P, _I, _D, _P, _P, _P, _PI, _PD, _P],
     "rpm_tridiag_spectra": [_P, _P, _I, _PI, _P, _P],

@@ -153,6 +153,15 @@ class BatchedPropagator:
                   int(values.shape[1]), float(lifetime_us), _lib.ptr(out), _lib.stream_handle())
         return out
 
+    def recombination(self):
+        """(kS, kT) shared by the batch's systems, or None (Hermitian propagation)."""
+        rates = {h.recombination_rates for h in self.hamiltonians}
+        if rates == {None}:
+            return None
+        if len(rates) != 1:
+            raise ValueError("all systems of a batch must have the same recombination rates")
+        return rates.pop()
+
     def propagate(self, initial_states, times_us, *, system_index: Sequence[int] | None = None,
                   lifetime_us: float | None = None, return_final_states: bool = False) -> BatchedResult:
         times = np.asarray(tuple(float(v) for v in times_us), dtype=float)
@@ -167,7 +176,16 @@ class BatchedPropagator:
         psi = self.load_states(initial_states, idx)
         values, errs, stats = self.propagate_device(psi, times, idx)
         yields = None
-        if lifetime_us is not None:
+        rates = self.recombination()
+        if rates is not None:
+            # singlet yield kS * int exp(-k_min t) P_S dt = (kS / k_min) * Simpson yield at tau = 1 / k_min
+            if lifetime_us is not None:
+                raise ValueError("with recombination rates the yield follows from the rates; omit lifetime_us")
+            k_min = min(rates)
+            if not k_min > 0.0:
+                raise ValueError("the smaller recombination rate must be positive for a yield")
+            yields = (rates[0] / k_min) * self.yields_device(times, values, 1.0 / k_min).cpu().numpy()
+        elif lifetime_us is not None:
             yields = self.yields_device(times, values, lifetime_us).cpu().numpy()
         vals = values.cpu().numpy()
         se = errs.cpu().numpy()

@@ -38,6 +38,7 @@ constexpr int kEwThreads = 256;
 constexpr int kEwPer = 8;                         // elements per thread
 constexpr int kEwChunk = kEwThreads * kEwPer;     // elements per block
 constexpr int kRecDoubles = 2 + kBMaxK + kBMaxK * kBMaxK;  // one spectra record (LD = kBMaxK)
+constexpr size_t kArnCtlSmem = sizeof(double2) * 3 * kBMaxK * kBMaxK;  // Arnoldi controller scratch
 
 struct TrajState {
   double t_now, dt, norm, new_norm2, acc_err, step_err, max_norm_err;
@@ -71,6 +72,13 @@ struct BatchDev {
   double* errs;     // [traj][ntimes]
   int nblk, gblk;
   int* active;      // trajectories not yet done
+  // Arnoldi (non-Hermitian systems: unequal recombination rates)
+  int arnoldi;
+  double grid_h;    // uniform observation spacing
+  double2* hess;    // [traj][kBMaxK + 1][kBMaxK] Hessenberg matrix H(i, j)
+  double2* hcur;    // [traj][kBMaxK] projections of the current Gram-Schmidt pass
+  double2* adots;   // [traj][nblk][kBMaxK] block partials of the projections
+  double2* expm;    // [traj][2][kBMaxK * kBMaxK] exp(-i H h) of T_M and T_(M-offset)
 };
 
 __device__ __forceinline__ bool traj_last_block(unsigned* counter) {
@@ -525,6 +533,267 @@ __global__ void __launch_bounds__(128) k_b_control(BatchDev B) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Arnoldi (non-Hermitian H: unequal recombination rates)
+// ---------------------------------------------------------------------------
+// Classical Gram-Schmidt, applied twice per iteration, of w = V_(j+1) (H v_j
+// from the passes) against v_0..v_j: projections in FP64 from FP32 products,
+// accumulated into column j of the Hessenberg matrix; the second pass's norm
+// gives H(j+1, j) and the scale of the next basis vector.
+__global__ void __launch_bounds__(kEwThreads) k_b_arn_dots(BatchDev B, int j, int pass) {
+  __shared__ double2 red[kEwThreads / 32][kBMaxK];
+  const int b = blockIdx.y;
+  TrajState& s = B.st[b];
+  if (s.skip) return;
+  const float2* base = B.V + (size_t)b * (B.m + 1) * B.ld;
+  const float2* w = base + (size_t)(j + 1) * B.ld;
+  const long long i0 = (long long)blockIdx.x * kEwChunk + threadIdx.x;
+  float2 wv[kEwPer];
+#pragma unroll
+  for (int k = 0; k < kEwPer; ++k) {
+    const long long e = i0 + (long long)k * kEwThreads;
+    wv[k] = e < s.n ? w[e] : make_float2(0.f, 0.f);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int i = 0; i <= j; ++i) {
+    const float2* v = base + (size_t)i * B.ld;
+    double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int k = 0; k < kEwPer; ++k) {
+      const long long e = i0 + (long long)k * kEwThreads;
+      if (e < s.n) {
+        const float2 q = v[e];  // conj(q) * w
+        acc.x += (double)q.x * wv[k].x + (double)q.y * wv[k].y;
+        acc.y += (double)q.x * wv[k].y - (double)q.y * wv[k].x;
+      }
+    }
+    acc.x = warp_sum(acc.x);
+    acc.y = warp_sum(acc.y);
+    if (lane == 0) red[warp][i] = acc;
+  }
+  __syncthreads();
+  double2* part = B.adots + ((size_t)b * B.nblk + blockIdx.x) * kBMaxK;
+  for (int i = threadIdx.x; i <= j; i += blockDim.x) {
+    double2 t = make_double2(0.0, 0.0);
+    for (int w2 = 0; w2 < kEwThreads / 32; ++w2) t = cadd(t, red[w2][i]);
+    part[i] = t;
+  }
+  if (traj_last_block(B.count + b)) {
+    for (int i = threadIdx.x; i <= j; i += blockDim.x) {
+      double2 t = make_double2(0.0, 0.0);
+      for (int k = 0; k < (int)gridDim.x; ++k) t = cadd(t, __ldcg(B.adots + ((size_t)b * B.nblk + k) * kBMaxK + i));
+      B.hcur[(size_t)b * kBMaxK + i] = t;
+      double2& h = B.hess[((size_t)b * (kBMaxK + 1) + i) * kBMaxK + j];
+      h = pass == 1 ? t : cadd(h, t);
+    }
+    if (threadIdx.x == 0) B.count[b] = 0;
+  }
+}
+
+__global__ void __launch_bounds__(kEwThreads) k_b_arn_axpy(BatchDev B, int j, int pass) {
+  __shared__ float2 hc[kBMaxK];
+  __shared__ double red[32];
+  const int b = blockIdx.y;
+  TrajState& s = B.st[b];
+  if (s.skip) return;
+  for (int i = threadIdx.x; i <= j; i += blockDim.x) {
+    const double2 t = B.hcur[(size_t)b * kBMaxK + i];
+    hc[i] = make_float2((float)t.x, (float)t.y);
+  }
+  __syncthreads();
+  float2* base = B.V + (size_t)b * (B.m + 1) * B.ld;
+  float2* w = base + (size_t)(j + 1) * B.ld;
+  double nn = 0.0;
+  const long long end = min(s.n, (long long)(blockIdx.x + 1) * kEwChunk);
+  for (long long e = (long long)blockIdx.x * kEwChunk + threadIdx.x; e < end; e += kEwThreads) {
+    float2 x = w[e];
+    for (int i = 0; i <= j; ++i) x = cfma(make_float2(-hc[i].x, -hc[i].y), base[(size_t)i * B.ld + e], x);
+    w[e] = x;
+    nn = fma((double)x.x, (double)x.x, fma((double)x.y, (double)x.y, nn));
+  }
+  if (pass != 2) return;
+  nn = block_sum(nn, red);
+  if (threadIdx.x == 0) B.part[((size_t)b * B.nblk + blockIdx.x) * 2] = nn;
+  if (traj_last_block(B.count + b) && threadIdx.x == 0) {
+    double tot = 0.0;
+    for (int k = 0; k < (int)gridDim.x; ++k) tot += __ldcg(B.part + ((size_t)b * B.nblk + k) * 2);
+    const double beta = sqrt(tot);
+    B.hess[((size_t)b * (kBMaxK + 1) + j + 1) * kBMaxK + j] = make_double2(beta, 0.0);
+    s.scale = beta > 0.0 ? 1.0 / beta : 0.0;
+    if (j + 1 < B.m) {
+      const double2 hd = B.hess[((size_t)b * (kBMaxK + 1) + j) * kBMaxK + j];
+      double ref = hypot(hd.x, hd.y);
+      if (j > 0) ref += B.hess[((size_t)b * (kBMaxK + 1) + j) * kBMaxK + j - 1].x;
+      if (!(beta > B.breakdown_rel * ref)) {
+        s.stop = 1;
+        s.skip = 1;
+        s.msize = j + 1;
+      }
+    }
+    B.count[b] = 0;
+  }
+}
+
+// Matrix product C = A X for n x n complex matrices in shared memory (row-major).
+__device__ void cmatmul(int n, const double2* A, const double2* X, double2* C) {
+  for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+    const int r = idx / n, c = idx - r * n;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int k = 0; k < n; ++k) acc = cfma(A[r * n + k], X[k * n + c], acc);
+    C[idx] = acc;
+  }
+  __syncthreads();
+}
+
+// E = exp(-i H h) for the leading n x n block of the Hessenberg matrix:
+// scaling and squaring with an 18-term Taylor polynomial (norm of the scaled
+// matrix at most 1/2: truncation below 1e-22).  P, Q, R: n x n scratch.
+__device__ void hessenberg_expm(const double2* hess, int n, double h, double2* P, double2* Q, double2* R,
+                                double2* out) {
+  __shared__ double s_norm;
+  for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+    const int r = idx / n, c = idx - r * n;
+    const double2 v = hess[(size_t)r * kBMaxK + c];
+    P[idx] = make_double2(v.y * h, -v.x * h);  // -i h H
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double best = 0.0;
+    for (int c = 0; c < n; ++c) {
+      double col = 0.0;
+      for (int r = 0; r < n; ++r) col += hypot(P[r * n + c].x, P[r * n + c].y);
+      best = fmax(best, col);
+    }
+    s_norm = best;
+  }
+  __syncthreads();
+  int sq = 0;
+  double scale = 1.0;
+  while (s_norm * scale > 0.5 && sq < 60) {
+    scale *= 0.5;
+    ++sq;
+  }
+  for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+    P[idx].x *= scale;
+    P[idx].y *= scale;
+    Q[idx] = make_double2((idx / n == idx % n) ? 1.0 : 0.0, 0.0);
+  }
+  __syncthreads();
+  // Horner: Q = I + P/1 (I + P/2 (I + ... (I + P/18)))
+  for (int k = 18; k >= 1; --k) {
+    cmatmul(n, P, Q, R);
+    const double inv = 1.0 / k;
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+      const bool diag = idx / n == idx % n;
+      Q[idx] = make_double2(R[idx].x * inv + (diag ? 1.0 : 0.0), R[idx].y * inv);
+    }
+    __syncthreads();
+  }
+  for (int t = 0; t < sq; ++t) {
+    cmatmul(n, Q, Q, R);
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) Q[idx] = R[idx];
+    __syncthreads();
+  }
+  for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) out[idx] = Q[idx];
+  __syncthreads();
+}
+
+// Arnoldi controller (one CTA per trajectory): exponentials of T_M and
+// T_(M-offset) over one observation spacing h, then marching c(k h) =
+// E^k e1 over the uniform observation grid; the step is the largest k h
+// whose embedded error (the reference's estimate, rpm_statevector_engine.py:
+// 690-715) meets budget * k h / T.  Every grid point of the step is an
+// observation point.  Dynamic shared memory: three kBMaxK^2 complex buffers.
+__global__ void __launch_bounds__(128) k_b_control_arn(BatchDev B) {
+  extern __shared__ double2 scratch[];
+  __shared__ double2 chi[kBMaxK], clo[kBMaxK], nhi[kBMaxK], nlo[kBMaxK];
+  __shared__ double red[32];
+  __shared__ int s_k;
+  const int b = blockIdx.x;
+  TrajState& s = B.st[b];
+  if (s.done) return;
+  const int M = s.msize;
+  const bool exact = s.stop != 0;
+  const int ML = max(1, M - B.offset);
+  double2* P = scratch;
+  double2* Q = P + kBMaxK * kBMaxK;
+  double2* R = Q + kBMaxK * kBMaxK;
+  double2* Ehi = B.expm + (size_t)b * 2 * kBMaxK * kBMaxK;
+  double2* Elo = Ehi + kBMaxK * kBMaxK;
+  const double* hess_d = reinterpret_cast<const double*>(B.hess + (size_t)b * (kBMaxK + 1) * kBMaxK);
+  hessenberg_expm(reinterpret_cast<const double2*>(hess_d), M, B.grid_h, P, Q, R, Ehi);
+  if (!exact) hessenberg_expm(reinterpret_cast<const double2*>(hess_d), ML, B.grid_h, P, Q, R, Elo);
+  const double t_now = s.t_now;
+  const double remaining = B.t_end - t_now;
+  const double dt_max = fmin(B.max_step, remaining);
+  int kmax = (int)floor(dt_max / B.grid_h + 1e-9);
+  kmax = min(kmax, kMaxPts);
+  kmax = min(kmax, B.ntimes - s.cursor);
+  for (int i = threadIdx.x; i < kBMaxK; i += blockDim.x) {
+    chi[i] = make_double2(i == 0 ? 1.0 : 0.0, 0.0);
+    clo[i] = chi[i];
+  }
+  if (threadIdx.x == 0) s_k = 0;
+  __syncthreads();
+  double2* rows = B.coef + (size_t)b * (kMaxPts + 1) * kBMaxK;
+  const double norm = s.norm;
+  for (int k = 1; k <= kmax; ++k) {
+    // threads 0-63: hi system, 64-127: lo system
+    const int t = threadIdx.x;
+    if (t < M) {
+      double2 acc = make_double2(0.0, 0.0);
+      for (int c = 0; c < M; ++c) acc = cfma(Ehi[t * M + c], chi[c], acc);
+      nhi[t] = acc;
+    } else if (t >= 64 && t - 64 < ML && !exact) {
+      const int r = t - 64;
+      double2 acc = make_double2(0.0, 0.0);
+      for (int c = 0; c < ML; ++c) acc = cfma(Elo[r * ML + c], clo[c], acc);
+      nlo[r] = acc;
+    }
+    __syncthreads();
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < M; i += blockDim.x) {
+      chi[i] = nhi[i];
+      if (!exact) {
+        if (i < ML) clo[i] = nlo[i];
+        const double2 lo = i < ML ? nlo[i] : make_double2(0.0, 0.0);
+        const double dx = nhi[i].x - lo.x, dy = nhi[i].y - lo.y;
+        acc = fma(dx, dx, fma(dy, dy, acc));
+      }
+    }
+    acc = block_sum(acc, red);
+    const double err = exact ? 0.0 : B.safety * norm * sqrt(acc);
+    const double tk = k * B.grid_h;
+    if (!(err <= B.budget * tk / B.t_end)) break;  // uniform: every thread sees the same sum
+    for (int i = threadIdx.x; i < kBMaxK; i += blockDim.x) rows[(size_t)(k - 1) * kBMaxK + i] = i < M ? chi[i] : make_double2(0.0, 0.0);
+    if (threadIdx.x == 0) {
+      B.perr[(size_t)b * kMaxPts + k - 1] = err;
+      s_k = k;
+      s.step_err = err;
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  const int kk = s_k;
+  if (kk == 0) {
+    if (threadIdx.x == 0) {
+      s.status = 3;  // the first observation spacing already exceeds the error budget
+      s.done = 1;
+      s.skip = 1;
+      atomicSub(B.active, 1);
+    }
+    return;
+  }
+  for (int i = threadIdx.x; i < kBMaxK; i += blockDim.x)
+    rows[(size_t)kMaxPts * kBMaxK + i] = rows[(size_t)(kk - 1) * kBMaxK + i];
+  if (threadIdx.x == 0) {
+    double dt = kk * B.grid_h;
+    if (remaining - dt < 1e-12) dt = remaining;
+    s.dt = dt;
+    s.npts = kk;
+  }
+}
+
 // psi = ||psi|| V c_end (FP64 accumulation); ||psi||^2 into new_norm2.
 __global__ void __launch_bounds__(kEwThreads) k_b_rebuild(BatchDev B) {
   __shared__ double2 cc[kBMaxK];
@@ -781,7 +1050,8 @@ static void free_graph(rpm_batch* B) {
 }
 
 struct Layout {
-  size_t st, V, coef, perr, part, count, gpart, ya, dotpart, dotcount, times, sysof, nof, active, total;
+  size_t st, V, coef, perr, part, count, gpart, ya, dotpart, dotcount, times, sysof, nof, active, hess, hcur, adots,
+      expm, total;
 };
 
 static Layout layout(const rpm_batch* B, int ntraj, int ntimes, int nblk, int gblk, int dot_blocks) {
@@ -807,6 +1077,10 @@ static Layout layout(const rpm_batch* B, int ntraj, int ntimes, int nblk, int gb
   L.sysof = take(sizeof(int) * ntraj);
   L.nof = take(sizeof(long long) * ntraj);
   L.active = take(sizeof(int));
+  L.hess = take(sizeof(double2) * (size_t)ntraj * (kBMaxK + 1) * kBMaxK);
+  L.hcur = take(sizeof(double2) * (size_t)ntraj * kBMaxK);
+  L.adots = take(sizeof(double2) * (size_t)ntraj * nblk * kBMaxK);
+  L.expm = take(sizeof(double2) * (size_t)ntraj * 2 * kBMaxK * kBMaxK);
   L.total = pos;
   return L;
 }
@@ -834,10 +1108,45 @@ static void record_step(rpm_batch* Bh, const BatchDev& B, const Layout& L, cudaS
   check_cuda(cudaStreamIsCapturing(st, &capturing), "capture status");
   const unsigned probe_flags = capturing == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : 0u;
   // The shape-specialised passes carry the Lanczos recurrence themselves
-  // (LanczosFuse: no update kernel); otherwise H psi + k_b_update.
+  // (LanczosFuse: no update kernel); otherwise H psi + k_b_update.  Non-
+  // Hermitian systems (unequal recombination rates) run Arnoldi instead.
   a.in = B.V;
   a.out = B.V + B.ld;
   const bool fused = cube_fast_usable(a, Bh->plan, ya);
+  if (B.arnoldi) {
+    if (!fused) fail(RPM_E_UNSUPPORTED, "unequal recombination rates need the shape-specialised H psi passes");
+    for (int j = 0; j < m; ++j) {
+      a.in = B.V + (size_t)j * B.ld;
+      a.out = B.V + (size_t)(j + 1) * B.ld;
+      LanczosFuse& z = a.lz;
+      z = LanczosFuse{};
+      z.on = 2;
+      z.first = j == 0;
+      z.last = j == m - 1;
+      z.j = j;
+      a.dot_out = nullptr;
+      a.dot_part = nullptr;
+      if (j == probe_j) check_cuda(cudaEventRecordWithFlags(Bh->probe0, st, probe_flags), "probe record");
+      if (!launch_cube_fast(a, Bh->plan, ya, B.ntraj, st)) fail(RPM_E_INVALID, "H psi passes unavailable");
+      if (j == probe_j) check_cuda(cudaEventRecordWithFlags(Bh->probe1, st, probe_flags), "probe record");
+      for (int pass = 1; pass <= 2; ++pass) {
+        k_b_arn_dots<<<ew, kEwThreads, 0, st>>>(B, j, pass);
+        k_b_arn_axpy<<<ew, kEwThreads, 0, st>>>(B, j, pass);
+      }
+    }
+    Bh->fused = false;
+    Bh->launches_per_step = 1 + 6 * m + 4;
+    check_cuda(cudaEventRecord(Bh->ev_fork, st), "fork record");
+    check_cuda(cudaStreamWaitEvent(Bh->side, Bh->ev_fork, 0), "fork wait");
+    k_b_gram<<<dim3(B.gblk, B.ntraj), 256, 0, Bh->side>>>(B);
+    check_cuda(cudaEventRecord(Bh->ev_join, Bh->side), "join record");
+    k_b_control_arn<<<B.ntraj, 128, kArnCtlSmem, st>>>(B);
+    k_b_rebuild<<<ew, kEwThreads, 0, st>>>(B);
+    check_cuda(cudaStreamWaitEvent(st, Bh->ev_join, 0), "join wait");
+    k_b_observe<<<B.ntraj, 256, sizeof(double2) * kBMaxK * kBMaxK, st>>>(B);
+    check_launch("batched Arnoldi step");
+    return;
+  }
   for (int j = 0; j < m; ++j) {
     a.in = B.V + (size_t)j * B.ld;
     a.out = B.V + (size_t)(j + 1) * B.ld;
@@ -945,6 +1254,29 @@ static void run_batch(rpm_batch* Bh, int ntraj, const int* sys_of, void* psi, co
   B.nblk = nblk;
   B.gblk = gblk;
   B.active = reinterpret_cast<int*>(base + L.active);
+  B.hess = reinterpret_cast<double2*>(base + L.hess);
+  B.hcur = reinterpret_cast<double2*>(base + L.hcur);
+  B.adots = reinterpret_cast<double2*>(base + L.adots);
+  B.expm = reinterpret_cast<double2*>(base + L.expm);
+  B.arnoldi = 0;
+  for (rpm_system* sy : Bh->systems) B.arnoldi |= sy->non_hermitian ? 1 : 0;
+  B.grid_h = 0.0;
+  if (B.arnoldi) {
+    // the Arnoldi controller marches over a uniform observation grid that
+    // starts at 0 or one spacing
+    if (ntimes < 2) fail(RPM_E_INVALID, "unequal recombination rates need at least two observation times");
+    const double h = times_host[1] - times_host[0];
+    const double k0 = times_host[0] / h;
+    if (!(h > 0.0) || !(std::fabs(k0) < 1e-9 || std::fabs(k0 - 1.0) < 1e-9))
+      fail(RPM_E_INVALID, "unequal recombination rates need observation times k h starting at 0 or h");
+    for (int k = 0; k < ntimes; ++k)
+      if (std::fabs(times_host[k] - (k + k0) * h) > 1e-9 * h * (k + 1))
+        fail(RPM_E_INVALID, "unequal recombination rates need uniformly spaced observation times");
+    B.grid_h = h;
+    check_cuda(cudaMemsetAsync(B.hess, 0, sizeof(double2) * (size_t)ntraj * (kBMaxK + 1) * kBMaxK, st), "memset hess");
+    check_cuda(cudaFuncSetAttribute(k_b_control_arn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kArnCtlSmem),
+               "Arnoldi control attr");
+  }
 
   k_b_setup<<<(ntraj + 127) / 128, 128, 0, st>>>(B, reinterpret_cast<const int*>(base + L.sysof),
                                                  reinterpret_cast<const long long*>(base + L.nof),

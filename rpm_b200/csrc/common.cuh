@@ -197,6 +197,13 @@ struct rpm_system {
   std::vector<int> lptr, lcol, rptr, rcol;
   std::vector<rpm::cd> lval, rval;
   rpm::cd pair[16];
+  // Haberkorn recombination with unequal rates (rpm_system_set_recombination):
+  // pair = pair_base - (i/2) |kS - kT| Q, Q = P_S (kS > kT) or P_T (kT > kS);
+  // the common decay exp(-min(kS, kT) t / 2) of the state is factored out.
+  rpm::cd pair_base[16];
+  bool recombination = false;
+  bool non_hermitian = false;
+  double rate_singlet = 0.0, rate_triplet = 0.0;
   std::vector<rpm::TermMeta> terms;
   std::vector<rpm::cd> ops;
   std::vector<int> coloff;

@@ -842,8 +842,17 @@ void launch_hpsi(rpm_system* sys, const T* in, T* out, int batch, long long ld, 
       a.ld = ld;
       a.views = cube_dev_of<T>(sys);
       rpm_system* one[1] = {sys};
-      launch_cube<T>(a, cube_plan(one, 1), ya, batch, stream);
-      return;
+      const CubePlan plan = cube_plan(one, 1);
+      // the general cube kernels keep only the real part of the pair diagonal:
+      // a non-Hermitian (recombination) system goes to the shape-specialised
+      // passes or to the CSR passes
+      if (!sys->non_hermitian) {
+        launch_cube<T>(a, plan, ya, batch, stream);
+        return;
+      }
+      if constexpr (std::is_same<T, float2>::value) {
+        if (launch_cube_fast(a, plan, ya, batch, stream)) return;
+      }
     }
     const SplitView<T>& s = split_of<T>(sys);
     bool a_ok = try_pass_a<T, 4>(s, in, ya, batch, ld, stream) || try_pass_a<T, 2>(s, in, ya, batch, ld, stream);
@@ -948,7 +957,7 @@ static void launch_hpsi_noalloc(rpm_system* sys, const T* in, T* out, int batch,
                                 " bytes exceeds its fixed 4 MiB scratch; use rpm_hpsi or a smaller batch");
   }
   T* ya = static_cast<T*>(noalloc_scratch());
-  if (sys->cube && sys->cube64.inner_l >= 1 && sys->cube64.inner_r >= 1) {
+  if (sys->cube && !sys->non_hermitian && sys->cube64.inner_l >= 1 && sys->cube64.inner_r >= 1) {
     HpsiArgs<T> a{};
     a.in = in;
     a.out = out;

@@ -16,6 +16,8 @@ namespace rpm {
 //          breakdown (beta_j <= breakdown_rel (|alpha_j| + beta_{j-1})).
 // Per-vector scalars of vector b live at ptr + b * dstride (doubles) or
 // ptr + b * istride (ints).
+// on == 2 (Arnoldi): pass R only scales (v_j = in * in_scale, written back,
+// no v_{j-1} term) and pass L stores H v_j unchanged, without reductions.
 struct LanczosFuse {
   int on, first, last, j;
   const float2* prev;  // v_{j-1} of vector b at prev + b * ld (unused when first)

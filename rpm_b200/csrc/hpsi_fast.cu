@@ -292,13 +292,14 @@ __global__ void __launch_bounds__(PassR<N1, NH>::WARPS * 32, 2)
   // fused Lanczos (j > 0): the tile receives w'_j and ptile v_{j-1}; below,
   // v_j = (w'_j - alpha_{j-1} v_{j-1}) * scale replaces w'_j in the tile and in `in`
   const bool combine = a.lz.on && !a.lz.first;
-  const float2* pv = combine ? a.lz.prev + (long long)b * a.ld : nullptr;
+  const bool with_prev = combine && a.lz.on == 1;  // Arnoldi (on == 2) only rescales
+  const float2* pv = with_prev ? a.lz.prev + (long long)b * a.ld : nullptr;
   for (int idx = threadIdx.x; idx < units; idx += NT) {
     int slot;
     long long g;
     unit_at(idx, slot, g);
     copy16(tile + slot, x_in + g);
-    if (combine) copy16(ptile + slot, pv + g);
+    if (with_prev) copy16(ptile + slot, pv + g);
   }
   for (int k = threadIdx.x; k < S::NTAB; k += NT) tab[k] = view->tabR[k];
   __syncthreads();
@@ -322,7 +323,7 @@ __global__ void __launch_bounds__(PassR<N1, NH>::WARPS * 32, 2)
   copy_wait_all();
   if (combine) {
     // each thread combines the units it copied (visible to it after its own wait)
-    const float al = (float)a.lz.alpha_prev[(long long)b * a.lz.dstride];
+    const float al = with_prev ? (float)a.lz.alpha_prev[(long long)b * a.lz.dstride] : 0.0f;
     const float sc = (float)in_scale(a, b);
     float2* xo = const_cast<float2*>(x_in);
     for (int idx = threadIdx.x; idx < units; idx += NT) {
@@ -330,7 +331,7 @@ __global__ void __launch_bounds__(PassR<N1, NH>::WARPS * 32, 2)
       long long g;
       unit_at(idx, slot, g);
       const float4 w = *reinterpret_cast<const float4*>(tile + slot);
-      const float4 q = *reinterpret_cast<const float4*>(ptile + slot);
+      const float4 q = with_prev ? *reinterpret_cast<const float4*>(ptile + slot) : make_float4(0.f, 0.f, 0.f, 0.f);
       float4 v;
       v.x = sc * fmaf(-al, q.x, w.x);
       v.y = sc * fmaf(-al, q.y, w.y);
@@ -477,10 +478,10 @@ __global__ void __launch_bounds__(PassL<N1, NH>::WARPS * 32, 2)
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int j = lane & 7, h = (lane >> 3) & 1, lg = lane >> 4, c = lane & 15;
-  const bool fused = a.lz.on != 0;
+  const bool fused = a.lz.on == 1;
   const bool has_prev = fused && !a.lz.first;
   const bool store = !fused || !a.lz.last;
-  const float sf = fused ? 1.0f : (float)in_scale(a, b);  // fused: pass R wrote the scaled v_j
+  const float sf = a.lz.on ? 1.0f : (float)in_scale(a, b);  // fused / Arnoldi: pass R wrote the scaled v_j
   const float bprev = has_prev ? (float)a.lz.beta_prev[(long long)b * a.lz.dstride] : 0.0f;
   // electron-pair operator rows of (e, h): eB-diagonal part merged, eB flip via the partner column
   float dp[2];
@@ -505,6 +506,13 @@ __global__ void __launch_bounds__(PassL<N1, NH>::WARPS * 32, 2)
   float din[2][4];
   float2 fin[2][4];
   cube_consts<S>(tab, din, fin);
+  // imaginary diagonal of the pair operator: nonzero only with unequal
+  // recombination rates (the non-Hermitian -(i/2) |kS - kT| Q term)
+  const bool cdiag = view->pair[0].y != 0.f || view->pair[5].y != 0.f || view->pair[10].y != 0.f ||
+                     view->pair[15].y != 0.f;
+  float gim[2];
+#pragma unroll
+  for (int e = 0; e < 2; ++e) gim[e] = view->pair[(e * 2 + h) * 4 + e * 2 + h].y;
   const float2* col = tile + c;
   const long long cofs = h * quarter + c0 + j;
   const float2* y_b = yb + (long long)b * (a.ya_ld ? a.ya_ld : a.ld) + cofs;
@@ -533,6 +541,7 @@ __global__ void __launch_bounds__(PassL<N1, NH>::WARPS * 32, 2)
       for (int i = 0; i < 4; ++i) {
         acc[e][i] = rmacf(rec.d[e] + dL[e] + din[e][i], x[e][i], make_float2(0.f, 0.f));
         acc[e][i] = cfma(cadd(cadd(rec.f[e], fL[e]), fin[e][i]), x[1 - e][i], acc[e][i]);
+        if (cdiag) acc[e][i] = cfma(make_float2(0.f, gim[e]), x[e][i], acc[e][i]);
       }
     cube_inner<S>(tab, x, acc);
     auto partner = [&](int delta, int dcol, const float2 (&cc)[2][2]) {
@@ -578,7 +587,7 @@ __global__ void __launch_bounds__(PassL<N1, NH>::WARPS * 32, 2)
     nv += (double)px;
   }
   if (fused) finish_lanczos(a, b, dot, nw, nv);
-  else if (a.dot_part) finish_dot_fast(a, b, dot);
+  else if (a.dot_part && !a.lz.on) finish_dot_fast(a, b, dot);
 }
 
 // ---------------------------------------------------------------------------
@@ -628,6 +637,7 @@ LaunchL pick_l(int n1, int nh) {
   if (n1 == 1 && nh == 5) return launch_l<1, 5>;
   if (n1 == 1 && nh == 6) return launch_l<1, 6>;
   if (n1 == 0 && nh == 6) return launch_l<0, 6>;
+  if (n1 == 1 && nh == 3) return launch_l<1, 3>;
   return nullptr;
 }
 LaunchR pick_r(int n1, int nh) {
@@ -638,6 +648,7 @@ LaunchR pick_r(int n1, int nh) {
   if (n1 == 1 && nh == 2) return launch_r<1, 2>;
   if (n1 == 2 && nh == 5) return launch_r<2, 5>;
   if (n1 == 0 && nh == 6) return launch_r<0, 6>;
+  if (n1 == 0 && nh == 3) return launch_r<0, 3>;
   return nullptr;
 }
 
@@ -686,7 +697,7 @@ bool cube_fast_usable(const HpsiArgs<float2>& a, const CubePlan& p, const float2
   const long long yld = a.ya_ld ? a.ya_ld : a.ld;
   auto aligned = [](const void* ptr) { return (reinterpret_cast<uintptr_t>(ptr) & 15u) == 0; };
   if ((a.ld & 1) || (yld & 1) || !aligned(a.in) || !aligned(a.out) || !aligned(ya)) return false;
-  if (a.lz.on && !a.lz.first && !aligned(a.lz.prev)) return false;
+  if (a.lz.on == 1 && !a.lz.first && !aligned(a.lz.prev)) return false;
   return pick_l(p.fl_n1, p.fl_nh) && pick_r(p.fr_n1, p.fr_nh);
 }
 

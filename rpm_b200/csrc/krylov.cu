@@ -565,6 +565,9 @@ int rpm_lanczos_basis(rpm_system* sys, const void* state_dev, int max_dim, doubl
     if (!sys || !state_dev || !basis_dev || !alpha_dev || !beta_dev || !actual_host || !norm_host)
       fail(RPM_E_INVALID, "NULL argument");
     if (!sys->on_device) fail(RPM_E_INVALID, "system was created host-only");
+    if (sys->non_hermitian)
+      fail(RPM_E_UNSUPPORTED, "Lanczos needs a Hermitian Hamiltonian; unequal recombination rates run on the "
+                              "batched propagator (Arnoldi)");
     lanczos_basis(sys, static_cast<const double2*>(state_dev), max_dim, breakdown_tol, static_cast<double2*>(basis_dev),
                   alpha_dev, beta_dev, actual_host, norm_host, static_cast<cudaStream_t>(stream));
   });

@@ -480,6 +480,56 @@ int rpm_system_info(const rpm_system* sys, long long* dimension, int* split, int
   });
 }
 
+int rpm_system_set_recombination(rpm_system* sys, double singlet_rate, double triplet_rate) {
+  return guarded([&] {
+    if (!sys) rpm::fail(RPM_E_INVALID, "system is NULL");
+    if (!sys->split) rpm::fail(RPM_E_UNSUPPORTED, "recombination needs a radical-split system");
+    if (!(singlet_rate >= 0.0) || !(triplet_rate >= 0.0) || !std::isfinite(singlet_rate) ||
+        !std::isfinite(triplet_rate))
+      rpm::fail(RPM_E_INVALID, "Recombination rates must be finite and nonnegative.");
+    if (!sys->recombination)
+      for (int k = 0; k < 16; ++k) sys->pair_base[k] = sys->pair[k];
+    // P_S on (eA, eB) in the order (uu, ud, du, dd): |S> = (|ud> - |du>) / sqrt 2
+    double ps[16] = {};
+    ps[1 * 4 + 1] = ps[2 * 4 + 2] = 0.5;
+    ps[1 * 4 + 2] = ps[2 * 4 + 1] = -0.5;
+    const bool singlet_faster = singlet_rate >= triplet_rate;
+    const double delta = std::fabs(singlet_rate - triplet_rate);
+    for (int k = 0; k < 16; ++k) {
+      const double q = singlet_faster ? ps[k] : ((k % 5 == 0) ? 1.0 : 0.0) - ps[k];  // P_T = 1 - P_S
+      sys->pair[k] = sys->pair_base[k] - rpm::cd(0.0, 0.5 * delta * q);
+    }
+    sys->recombination = true;
+    sys->non_hermitian = delta > 0.0;
+    sys->rate_singlet = singlet_rate;
+    sys->rate_triplet = triplet_rate;
+    if (sys->on_device) {
+      for (int k = 0; k < 16; ++k) {
+        const double2 v = make_double2(sys->pair[k].real(), sys->pair[k].imag());
+        sys->split64.pair[k] = v;
+        sys->split32.pair[k] = make_float2((float)v.x, (float)v.y);
+        sys->cube64.pair[k] = v;
+        sys->cube32.pair[k] = make_float2((float)v.x, (float)v.y);
+      }
+      if (sys->cube) {
+        rpm::check_cuda(cudaMemcpy(sys->cube64_dev, &sys->cube64, sizeof(sys->cube64), cudaMemcpyHostToDevice),
+                   "update cube view");
+        rpm::check_cuda(cudaMemcpy(sys->cube32_dev, &sys->cube32, sizeof(sys->cube32), cudaMemcpyHostToDevice),
+                   "update cube view");
+      }
+    }
+  });
+}
+
+int rpm_system_recombination(const rpm_system* sys, double* singlet_rate, double* triplet_rate, int* non_hermitian) {
+  return guarded([&] {
+    if (!sys) rpm::fail(RPM_E_INVALID, "system is NULL");
+    if (singlet_rate) *singlet_rate = sys->rate_singlet;
+    if (triplet_rate) *triplet_rate = sys->rate_triplet;
+    if (non_hermitian) *non_hermitian = sys->non_hermitian ? 1 : 0;
+  });
+}
+
 int rpm_system_split_tables(const rpm_system* sys, int* lptr, int* lcol, double* lval, int* rptr, int* rcol,
                             double* rval, long long* offl, long long* offr, double* pair) {
   return guarded([&] {

@@ -106,6 +106,11 @@ class _DeviceSystem:
         _lib.call("rpm_system_info", handle, *[ctypes.byref(v) for v in info])
         self.n, self.split, self.nl, self.nr, self.nnz_l, self.nnz_r = (v.value for v in info)
 
+    def recombination(self):
+        ks, kt, nh = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        _lib.call("rpm_system_recombination", self.handle, ctypes.byref(ks), ctypes.byref(kt), ctypes.byref(nh))
+        return ks.value, kt.value, bool(nh.value)
+
     @property
     def fast_hpsi(self) -> bool:
         """True when complex64 H psi runs on the shape-specialised kernels."""
@@ -204,6 +209,28 @@ class MatrixFreeHamiltonian:
         split = _auto_split(self.dimensions, self.terms) if _split is True else (_split or None)
         self._system = _DeviceSystem(self.dimensions, self.terms, *(split or ((), ())),
                                      tolerance=hermitian_tolerance)
+
+    # -- recombination (batched path) ------------------------------------------
+    def set_recombination_rates(self, singlet_rate: float, triplet_rate: float) -> None:
+        """Haberkorn recombination rates (1/us) for the batched propagator.
+
+        The state evolves under H - (i/2)(kS P_S + kT P_T).  The common decay
+        exp(-min(kS, kT) t / 2) is factored out: the batched propagator reports
+        singlet populations of the factored state and singlet yields
+        kS * integral exp(-min(kS, kT) t) P_S(t) dt (for kS = kT = 1/tau the
+        reference's yield).  With kS != kT H psi becomes non-Hermitian
+        (``matvec`` applies the factored operator) and only the batched
+        propagator (Arnoldi) accepts the system.  Set before building a batch.
+        """
+        if self._system.split == 0:
+            raise ValueError("recombination rates need a radical-split Hamiltonian")
+        _lib.call("rpm_system_set_recombination", self._system.handle, float(singlet_rate), float(triplet_rate))
+
+    @property
+    def recombination_rates(self):
+        """(singlet rate, triplet rate) in 1/us, or None when not set."""
+        ks, kt, _ = self._system.recombination()
+        return None if ks == 0.0 and kt == 0.0 else (ks, kt)
 
     # -- GPU-native interface ------------------------------------------------
     def apply(self, psi, out, *, batch: int = 1, precision: int = 128, stream=None) -> None:
