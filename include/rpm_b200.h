@@ -273,7 +273,64 @@ int rpm_batch_propagate(rpm_batch* batch, int ntraj, const int* sys_of_host, voi
  * finished. */
 int rpm_batch_counters(rpm_batch* batch, int reset, long long* kernel_launches, long long* step_replays,
                        double* hpsi_ms_mean, long long* hpsi_samples);
+/* Replace the configured state-error budget for later propagate calls (the
+ * knob ENG:620-649 exposes as a mutable attribute). */
+int rpm_batch_set_budget(rpm_batch* batch, double state_error_budget);
 int rpm_batch_destroy(rpm_batch* batch);
+
+/* -------------------------------------------------------------------------
+ * Adjoint sweep for gradients of the singlet yield.  No reference
+ * counterpart: the reference's only derivatives are finite differences of
+ * yields over angle grids (np.gradient over theta,
+ * rpm_quantum_needle_reproduction.py and rpm_three_nitrogen_quadrupole.py:153);
+ * this replaces central differences through ENG:717-933.
+ * The yield is Phi = sum_k w_k <psi_k|P_S|psi_k> on a uniform grid
+ * t_k = t_0 + k dt, psi_{k+1} = exp(-i H_k dt) psi_k (equal recombination
+ * rates, decay folded into w_k).  The adjoint lambda_k = U_k^dag lambda_{k+1}
+ * + w_k P_S psi_k is marched backwards and, per interval,
+ *   M_ab += int <lambda| (|a><b| (x) 1) |psi> dt   (a, b = 2 eA + eB),
+ *   S_r  += int <lambda| D_r |psi> dt            (derivative systems D_r),
+ *   W    += int <lambda| H |psi> dt              (FP64, optional),
+ * so that dPhi/dp = 2 Im( sum_ab E_ab M_ab + sum_r c_r S_r + c_H W ) for
+ * dH/dp = E (x) 1 + sum_r c_r D_r + c_H H.  The first two state axes must be
+ * the electrons; systems must be Hermitian radical-split cube-form systems.
+ * ------------------------------------------------------------------------- */
+typedef struct rpm_adjoint rpm_adjoint;
+
+/* Workspace for ntraj trajectories of dimension n (states spaced ld
+ * elements, ld even); `degree` Taylor terms per interval (1..24),
+ * `nodes` Gauss-Legendre nodes (1..4) and the basis precision
+ * (RPM_PREC_C64 or RPM_PREC_C128; states stay FP64). */
+int rpm_adjoint_create(int ntraj, long long n, long long ld, int degree, int nodes, int precision,
+                       rpm_adjoint** out);
+int rpm_adjoint_destroy(rpm_adjoint* adj);
+/* lambda += weight * P_S psi for every trajectory (complex128 device buffers). */
+int rpm_adjoint_source(rpm_adjoint* adj, const void* psi_dev, void* lambda_dev, double weight, void* stream);
+/* Walk intervals j = nintervals-1 .. 0 backwards.  On entry lambda_dev /
+ * psi_dev (ntraj x ld complex128) hold lambda and psi at the end of interval
+ * nintervals-1 (lambda including its source there); on return they hold them
+ * at the start of interval 0, lambda including source_weights[0].  Interval
+ * j evolves under systems[segment_of_interval[j]] (host arrays).
+ * density_dev: ntraj x nseg x 16 complex (FP64, accumulated);
+ * derivative_dev: ntraj x nseg x nder complex (accumulated), with
+ * derivative_systems[s * nder + r] (NULL: none) applied in segment s;
+ * energy_dev (optional): ntraj x nseg complex, accumulated W.
+ * *max_tail (optional; synchronises the stream) receives the largest
+ * ||last Taylor term|| / ||psi|| over all intervals and trajectories. */
+int rpm_adjoint_sweep(rpm_adjoint* adj, rpm_system* const* systems, int nseg,
+                      rpm_system* const* derivative_systems, int nder, const int* segment_of_interval,
+                      const double* source_weights, double dt, int nintervals, void* lambda_dev,
+                      void* psi_dev, double* density_dev, double* derivative_dev, double* energy_dev,
+                      double* max_tail, void* stream);
+/* Forward Taylor stepping with the same basis: psi_dev (ntraj x ld
+ * complex128) advances over `nintervals` intervals of length dt (interval j
+ * under systems[segment_of_interval[j]]); populations_dev[b * pop_ld + j]
+ * receives the singlet population at the end of interval j (ENG:492-497).
+ * A fixed schedule, so yields are smooth in the Hamiltonian's parameters
+ * (finite differences through it need no frozen step controller). */
+int rpm_adjoint_forward(rpm_adjoint* adj, rpm_system* const* systems, int nseg, const int* segment_of_interval,
+                        double dt, int nintervals, void* psi_dev, double* populations_dev, long long pop_ld,
+                        double* max_tail, void* stream);
 
 #ifdef __cplusplus
 }

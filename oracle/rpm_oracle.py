@@ -830,3 +830,49 @@ def haberkorn_dense(h_dense, dimensions: Sequence[int], psi0, times_us, singlet_
     factored = pops * np.exp(kmin * times)
     yield_value = singlet_rate * simpson(pops, times)
     return factored, yield_value
+
+
+# ---------------------------------------------------------------------------
+# Square field pulse and yield gradients (no reference implementation: dense
+# restatement of the segment loop of rpm_nuclear_spin_rotation_control.py:
+# 281-308 with per-segment Hamiltonians, and central differences through it)
+# ---------------------------------------------------------------------------
+def pulsed_yield_dense(h_static, h_pulse, dimensions: Sequence[int], psi0, times_us, pulse_start_us: float,
+                       pulse_end_us: float, lifetime_us: float):
+    """Singlet populations on a uniform grid and the Simpson yield (JD:418-420)
+    for a piecewise-constant Hamiltonian: ``h_pulse`` on observation intervals
+    inside [pulse_start, pulse_end], ``h_static`` elsewhere (dense expm of each
+    interval propagator; pulse edges on grid points)."""
+    from scipy.linalg import expm
+
+    dims = tuple(int(v) for v in dimensions)
+    t = np.asarray(times_us, dtype=float)
+    dt = float(t[1] - t[0])
+    props = (expm(-1j * np.asarray(h_static, dtype=complex) * dt), expm(-1j * np.asarray(h_pulse, dtype=complex) * dt))
+    psi = np.asarray(psi0, dtype=complex).copy()
+    pops = np.empty(t.size)
+    pops[0] = singlet_population(psi, dims)
+    for k in range(t.size - 1):
+        mid = 0.5 * (t[k] + t[k + 1])
+        psi = props[1 if pulse_start_us < mid < pulse_end_us else 0] @ psi
+        pops[k + 1] = singlet_population(psi, dims)
+    return pops, integrate_yield(t, pops, lifetime_us)
+
+
+def central_difference(function, params, relative_step: float = 1e-4, richardson: bool = False) -> np.ndarray:
+    """Central differences of a scalar function, step relative_step * max(|p|, 1);
+    with ``richardson`` the steps h and h/2 are combined, (4 D(h/2) - D(h)) / 3,
+    which cancels the O(h^2) truncation term."""
+    p = np.asarray(params, dtype=float)
+    out = np.empty(p.size)
+    for i in range(p.size):
+        h = relative_step * max(abs(p[i]), 1.0)
+
+        def diff(step):
+            up, down = p.copy(), p.copy()
+            up[i] += step
+            down[i] -= step
+            return (function(up) - function(down)) / (2.0 * step)
+
+        out[i] = (4.0 * diff(0.5 * h) - diff(h)) / 3.0 if richardson else diff(h)
+    return out

@@ -103,7 +103,14 @@ SIGNATURES: dict[str, list] = {
     "rpm_batch_leading_dimension": [_P, _PLL],
     "rpm_batch_propagate": [_P, _I, _PI, _P, _PD, _I, _P, _P, ctypes.POINTER(rpm_batch_stats), _P],
     "rpm_batch_destroy": [_P],
+    "rpm_batch_set_budget": [_P, _D],
     "rpm_batch_counters": [_P, _I, _PLL, _PLL, _PD, _PLL],
+    "rpm_adjoint_create": [_I, _LL, _LL, _I, _I, _I, ctypes.POINTER(_P)],
+    "rpm_adjoint_destroy": [_P],
+    "rpm_adjoint_source": [_P, _P, _P, _D, _P],
+    "rpm_adjoint_sweep": [_P, ctypes.POINTER(_P), _I, ctypes.POINTER(_P), _I, _PI, _PD, _D, _I, _P, _P, _P, _P,
+                          _P, _PD, _P],
+    "rpm_adjoint_forward": [_P, ctypes.POINTER(_P), _I, _PI, _D, _I, _P, _P, _LL, _PD, _P],
 }
 
 _lib = None

@@ -136,6 +136,10 @@ class BatchedPropagator:
                   int(times.size), _lib.ptr(values), _lib.ptr(errs), stats, _lib.stream_handle(stream))
         return values, errs, stats
 
+    def set_state_error_budget(self, budget: float) -> None:
+        """Budget of later propagate calls (ENG:620-649 keeps it mutable too)."""
+        _lib.call("rpm_batch_set_budget", self._handle, float(budget))
+
     def counters(self, reset: bool = False) -> dict:
         """Kernel launches, Krylov-step replays and the mean batched H psi time (ms)."""
         k, r, n = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()

@@ -1421,6 +1421,14 @@ int rpm_batch_counters(rpm_batch* batch, int reset, long long* kernel_launches, 
   });
 }
 
+int rpm_batch_set_budget(rpm_batch* batch, double state_error_budget) {
+  return guarded([&] {
+    if (!batch) fail(RPM_E_INVALID, "batch is NULL");
+    if (!(state_error_budget > 0.0)) fail(RPM_E_INVALID, "the state-error budget must be positive");
+    batch->cfg.state_error_budget = state_error_budget;
+  });
+}
+
 int rpm_batch_destroy(rpm_batch* batch) {
   return guarded([&] {
     if (!batch) return;

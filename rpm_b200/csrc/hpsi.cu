@@ -865,6 +865,30 @@ void launch_hpsi(rpm_system* sys, const T* in, T* out, int batch, long long ld, 
   launch_generic<T>(generic_of<T>(sys), in, out, batch, ld, stream);
 }
 
+template <class T>
+void launch_hpsi_scaled(rpm_system* sys, const T* in, T* out, int batch, long long ld, const double* scale_dev,
+                        cudaStream_t stream) {
+  if (!sys->on_device) fail(RPM_E_INVALID, "system was created host-only");
+  if (!sys->split || !sys->cube || sys->cube64.inner_l < 1 || sys->cube64.inner_r < 1 || sys->non_hermitian)
+    fail(RPM_E_UNSUPPORTED,
+         "scaled H psi needs a Hermitian radical-split system with a trailing spin-1/2 digit per radical");
+  if (batch < 1) return;
+  T* ya = static_cast<T*>(system_scratch(sys, SLOT_YA, (size_t)batch * ld * sizeof(T)));
+  HpsiArgs<T> a{};
+  a.in = in;
+  a.out = out;
+  a.ld = ld;
+  a.in_scale = scale_dev;
+  a.scale_stride = 0;
+  a.views = cube_dev_of<T>(sys);
+  rpm_system* one[1] = {sys};
+  launch_cube<T>(a, cube_plan(one, 1), ya, batch, stream);
+}
+
+template void launch_hpsi_scaled<float2>(rpm_system*, const float2*, float2*, int, long long, const double*,
+                                         cudaStream_t);
+template void launch_hpsi_scaled<double2>(rpm_system*, const double2*, double2*, int, long long, const double*,
+                                          cudaStream_t);
 template void launch_hpsi<double2>(rpm_system*, const double2*, double2*, int, long long, cudaStream_t);
 template void launch_hpsi<float2>(rpm_system*, const float2*, float2*, int, long long, cudaStream_t);
 template void launch_cube<double2>(const HpsiArgs<double2>&, const CubePlan&, double2*, int, cudaStream_t);

@@ -77,5 +77,10 @@ bool cube_fast_usable(const HpsiArgs<float2>& a, const CubePlan& p, const float2
 // Two passes: pass L into `ya` (batch x ld scratch), pass R into a.out.
 template <class T>
 void launch_cube(const HpsiArgs<T>& a, const CubePlan& p, T* ya, int batch, cudaStream_t stream);
+// out = H (in * scale_dev[0]) for `batch` vectors of one Hermitian cube-form
+// system (every vector uses the same device scale).
+template <class T>
+void launch_hpsi_scaled(rpm_system* sys, const T* in, T* out, int batch, long long ld, const double* scale_dev,
+                        cudaStream_t stream);
 
 }  // namespace rpm
