@@ -9,6 +9,7 @@ namespace rpm {
 // when `on` is 0).  Iteration j of vector b, in Paige's ordering:
 //   pass R stages v_j = (w'_j - alpha_{j-1} v_{j-1}) * in_scale (j > 0) from
 //          `in` (holding w'_j) and `prev`, and writes v_j back into `in`;
+//   pass R also subtracts beta_{j-1} v_{j-1} from its partial;
 //   pass L writes w'_{j+1} = H v_j - beta_{j-1} v_{j-1} into `out` (not for
 //          the last iteration) and reduces <v_j, w'>, |w'|^2 and |v_j|^2;
 //          its last block sets alpha_j = <v_j, w'> / |v_j|^2 and

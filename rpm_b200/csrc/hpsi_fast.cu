@@ -28,8 +28,11 @@
 // staged tile (conflict-free: padded rows in pass R, 128-byte rows in pass L).
 // Pass R stores its partial row-wise (each lane 32 contiguous bytes); pass L
 // reads it column-coalesced, prefetched at the start of each task, and fuses
-// <psi, H psi>.  Pass L walks the batch in reverse order so that the partials
-// and inputs written or read last are still in L2 when it starts.
+// <psi, H psi>.  In the fused Lanczos iteration pass R also subtracts
+// beta_{j-1} v_{j-1} (staged there for the combine) from the partial, so
+// pass L never reads v_{j-1}.  Pass L walks the batch in reverse order so
+// that the partials and inputs written or read last are still in L2 when it
+// starts.
 #include <utility>
 #include <vector>
 
@@ -346,7 +349,10 @@ __global__ void __launch_bounds__(PassR<N1, NH>::WARPS * 32, 2)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int row = lane & 15, hsel = lane >> 4;
   const float sf = a.lz.on ? 1.0f : (float)in_scale(a, b);  // fused: the staged v_j is already scaled
+  // Paige's -beta_{j-1} v_{j-1} joins the partial here, where v_{j-1} is staged
+  const float bprev = with_prev ? (float)a.lz.beta_prev[(long long)b * a.lz.dstride] : 0.0f;
   const float2* rowp = tile + row * RS;
+  const float2* prowp = ptile + row * RS;
   float din[2][4];
   float2 fin[2][4];
   cube_consts<S>(tab, din, fin);
@@ -404,6 +410,18 @@ __global__ void __launch_bounds__(PassR<N1, NH>::WARPS * 32, 2)
         w1.y = sf * acc[e][2].y;
         w1.z = sf * acc[e][3].x;
         w1.w = sf * acc[e][3].y;
+        if (with_prev) {
+          const float4 q0 = *reinterpret_cast<const float4*>(prowp + e * HR + 4 * o);
+          const float4 q1 = *reinterpret_cast<const float4*>(prowp + e * HR + 4 * o + 2);
+          w0.x = fmaf(-bprev, q0.x, w0.x);
+          w0.y = fmaf(-bprev, q0.y, w0.y);
+          w0.z = fmaf(-bprev, q0.z, w0.z);
+          w0.w = fmaf(-bprev, q0.w, w0.w);
+          w1.x = fmaf(-bprev, q1.x, w1.x);
+          w1.y = fmaf(-bprev, q1.y, w1.y);
+          w1.z = fmaf(-bprev, q1.z, w1.z);
+          w1.w = fmaf(-bprev, q1.w, w1.w);
+        }
         *reinterpret_cast<float4*>(y_b + at) = w0;
         *reinterpret_cast<float4*>(y_b + at + 2) = w1;
       }
@@ -479,10 +497,8 @@ __global__ void __launch_bounds__(PassL<N1, NH>::WARPS * 32, 2)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int j = lane & 7, h = (lane >> 3) & 1, lg = lane >> 4, c = lane & 15;
   const bool fused = a.lz.on == 1;
-  const bool has_prev = fused && !a.lz.first;
   const bool store = !fused || !a.lz.last;
   const float sf = a.lz.on ? 1.0f : (float)in_scale(a, b);  // fused / Arnoldi: pass R wrote the scaled v_j
-  const float bprev = has_prev ? (float)a.lz.beta_prev[(long long)b * a.lz.dstride] : 0.0f;
   // electron-pair operator rows of (e, h): eB-diagonal part merged, eB flip via the partner column
   float dp[2];
   float2 fp[2], pp[2][2];
@@ -517,19 +533,15 @@ __global__ void __launch_bounds__(PassL<N1, NH>::WARPS * 32, 2)
   const long long cofs = h * quarter + c0 + j;
   const float2* y_b = yb + (long long)b * (a.ya_ld ? a.ya_ld : a.ld) + cofs;
   float2* y_out = a.out + (long long)b * a.ld + cofs;
-  const float2* y_p = has_prev ? a.lz.prev + (long long)b * a.ld + cofs : nullptr;
   double dot = 0.0, nw = 0.0, nv = 0.0;
   for (int o = warp; o < NO; o += P::WARPS) {
     const ORec rec = orec[o];
     const int lo = o * 8 + lg * 4;  // l of cube element i = 0
-    float2 pb[2][4], pp4[2][4];  // pass-R partial and v_{j-1} of the cube, loaded early
+    float2 pb[2][4];  // pass-R partial of the cube (with -beta_{j-1} v_{j-1} when fused), loaded early
 #pragma unroll
     for (int e = 0; e < 2; ++e)
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        pb[e][i] = __ldcg(y_b + 2 * e * quarter + (long long)(lo + i) * HR);
-        pp4[e][i] = has_prev ? __ldcg(y_p + 2 * e * quarter + (long long)(lo + i) * HR) : make_float2(0.f, 0.f);
-      }
+      for (int i = 0; i < 4; ++i) pb[e][i] = __ldcg(y_b + 2 * e * quarter + (long long)(lo + i) * HR);
     float2 x[2][4], acc[2][4];
 #pragma unroll
     for (int e = 0; e < 2; ++e)
@@ -572,11 +584,7 @@ __global__ void __launch_bounds__(PassL<N1, NH>::WARPS * 32, 2)
       for (int i = 0; i < 4; ++i) {
         float2 v;
         v.x = fmaf(sf, acc[e][i].x, pb[e][i].x);
-        v.y = fmaf(sf, acc[e][i].y, pb[e][i].y);
-        if (has_prev) {  // Paige: w' = H v_j - beta_{j-1} v_{j-1}
-          v.x = fmaf(-bprev, pp4[e][i].x, v.x);
-          v.y = fmaf(-bprev, pp4[e][i].y, v.y);
-        }
+        v.y = fmaf(sf, acc[e][i].y, pb[e][i].y);  // fused: w' = H v_j - beta_{j-1} v_{j-1}
         if (store) y_out[2 * e * quarter + (long long)(lo + i) * HR] = v;
         part = fmaf(x[e][i].x, v.x, fmaf(x[e][i].y, v.y, part));
         pw = fmaf(v.x, v.x, fmaf(v.y, v.y, pw));
