@@ -256,6 +256,45 @@ def hpsi_probe(args) -> None:
                       "ms_per_launch_pair": ms, "algorithmic_GBps": gbs, "hbm_frac": gbs / peak}), flush=True)
 
 
+def adjoint_sample(full, direction, dev, vectors: int = 16, horizon_us: float = 1.0):
+    """Yield gradients (|B|, theta, phi, pulse amplitude, hyperfine scale) of
+    `vectors` random-phase trajectories of the full system with a 300 nT
+    transverse pulse on [0.2, 0.7] us, timed forward + backward on the device
+    for both adjoint precisions; a side measurement next to the main line."""
+    import numpy as np
+    import torch
+
+    from rpm_b200 import adjoint, synthetic
+
+    params = np.array([50.0, direction[0], direction[1], 300.0, 1.0])
+    model = adjoint.ParametricRadicalPair(full, pulse_start_us=0.2, pulse_duration_us=0.5)
+    times = np.arange(int(round(horizon_us / GRID_US)) + 1) * GRID_US
+    states = list(synthetic.random_phase_vectors(full.dimensions, vectors, 4242))
+    out = {"metric": "adjoint yield-gradient throughput, 5 parameters", "unit": "trajectory-us/s",
+           "sample": f"{vectors} trajectories x {horizon_us:g} us (221,184 dims, 300 nT pulse on [0.2, 0.7] us)"}
+    try:
+        for precision in ("c128", "c64"):
+            engine = adjoint.AdjointYieldGradient(model, precision=precision)
+            torch.cuda.synchronize(dev)
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record()
+            fwd = engine.forward(params, states, times, LIFETIME_US)
+            e1.record()
+            grads, diag = engine.backward(params, fwd)
+            e2.record()
+            torch.cuda.synchronize(dev)
+            fwd["workspace"].close()
+            total = e0.elapsed_time(e2) / 1e3
+            out[precision] = {"value": vectors * horizon_us / total, "forward_s": e0.elapsed_time(e1) / 1e3,
+                              "backward_s": e1.elapsed_time(e2) / 1e3, "taylor_degree": diag["taylor_degree"],
+                              "max_taylor_tail": diag["max_taylor_tail"],
+                              "checkpoint_drift": diag["checkpoint_drift"],
+                              "mean_gradient": [float(v) for v in grads.mean(axis=0)]}
+    except Exception as exc:  # a side measurement must not sink the main line
+        out["error"] = f"{type(exc).__name__}: {exc}"
+    return out
+
+
 def b200_arm(args, rank: int, world: int, dist) -> None:
     import numpy as np
     import torch
@@ -396,6 +435,9 @@ def b200_arm(args, rank: int, world: int, dist) -> None:
             cpu = {"value": cpu_value, "unit": UNIT, "cores": base.workers, "kind": "port",
                    "sample": f"{base.workers} trajectories x {args.cpu_horizon} us prefix (Krylov 8-40, budget "
                              f"1e-10 scaled), extrapolated to 5 us; {per_traj:.1f} s each"}
+        adjoint = None
+        if world == 1 and not args.no_adjoint:
+            adjoint = adjoint_sample(full, dirs[0], dev)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
@@ -421,6 +463,7 @@ def b200_arm(args, rank: int, world: int, dist) -> None:
             "batched_over_plain": value / world / plain["value"] if plain else None,
             "yield_err_vs_fp64": y_err,
             "yields_gathered": int(yields_all.numel()),
+            "adjoint": adjoint,
         }
     if line is not None:
         print(json.dumps(line), flush=True)
@@ -441,6 +484,7 @@ def main() -> None:
     p.add_argument("--cpu-horizon", type=float, default=0.025, help="us of the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison trajectory")
+    p.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-gradient side measurement")
     p.add_argument("--horizon", type=float, default=HORIZON_US,
                    help="propagation horizon in us (5 us is the benchmark workload; shorter only for profiling)")
     p.add_argument("--hpsi-only", type=int, default=0, metavar="K",
