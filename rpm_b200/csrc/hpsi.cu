@@ -420,6 +420,19 @@ __global__ void __launch_bounds__(256) cube_pass_l(HpsiArgs<T> a, T* __restrict_
       }
     cube_apply<T, NI>(side, sm.tab, ic, rec, dout, fout, x, acc,
                       [&](int e, int i, int delta) { return cb[(e * C + i) * plane + delta * W]; });
+    // imaginary diagonal of the pair operator: nonzero only with unequal
+    // recombination rates (the non-Hermitian -(i/2) |kS - kT| Q term)
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const R g = (R)pair[(e * 2 + h) * 4 + e * 2 + h].y;
+      if (g != (R)0) {
+#pragma unroll
+        for (int i = 0; i < C; ++i) {
+          acc[e][i].x -= g * x[e][i].y;
+          acc[e][i].y += g * x[e][i].x;
+        }
+      }
+    }
     const T* cp = cb + (h ? -TR : TR);  // partner column: electron B flipped
 #pragma unroll
     for (int ep = 0; ep < 2; ++ep) {
@@ -842,17 +855,8 @@ void launch_hpsi(rpm_system* sys, const T* in, T* out, int batch, long long ld, 
       a.ld = ld;
       a.views = cube_dev_of<T>(sys);
       rpm_system* one[1] = {sys};
-      const CubePlan plan = cube_plan(one, 1);
-      // the general cube kernels keep only the real part of the pair diagonal:
-      // a non-Hermitian (recombination) system goes to the shape-specialised
-      // passes or to the CSR passes
-      if (!sys->non_hermitian) {
-        launch_cube<T>(a, plan, ya, batch, stream);
-        return;
-      }
-      if constexpr (std::is_same<T, float2>::value) {
-        if (launch_cube_fast(a, plan, ya, batch, stream)) return;
-      }
+      launch_cube<T>(a, cube_plan(one, 1), ya, batch, stream);
+      return;
     }
     const SplitView<T>& s = split_of<T>(sys);
     bool a_ok = try_pass_a<T, 4>(s, in, ya, batch, ld, stream) || try_pass_a<T, 2>(s, in, ya, batch, ld, stream);

@@ -114,3 +114,33 @@ def test_arnoldi_full_size_near_equal_rates_match_lanczos():
                                                                                           lifetime_us=1.0)
     assert np.max(np.abs(a.observable_values - l.observable_values)) < 1e-5
     assert np.max(np.abs(a.yields - l.yields)) < 1e-6
+
+
+@pytest.mark.gpu
+def test_non_hermitian_action_on_the_general_cube_kernels():
+    """A layout without shape-specialised passes (96 dimensions): complex128 and complex64 H psi."""
+    import torch
+
+    import rpm_b200 as rb
+    from rpm_b200 import synthetic
+
+    sysm = synthetic.small_system()
+    terms = sysm.terms(0.4, 1.1)
+    h = rb.CompiledFullPairHamiltonian(sysm.dimensions, terms, left_axes=sysm.left_axes, right_axes=sysm.right_axes)
+    assert not h._system.fast_hpsi
+    dense = oracle.MatrixFreeHamiltonian(sysm.dimensions, [oracle.LocalTerm(t.axes, t.operator) for t in terms]).explicit_matrix()
+    ks, kt = 1.0, 2.0
+    h.set_recombination_rates(ks, kt)
+    m = math.prod(sysm.dimensions) // 4
+    ps4 = np.zeros((4, 4), dtype=complex)
+    ps4[1, 1] = ps4[2, 2] = 0.5
+    ps4[1, 2] = ps4[2, 1] = -0.5
+    expected_op = dense - 0.5j * (kt - ks) * np.kron(np.eye(4) - ps4, np.eye(m))
+    rng = np.random.default_rng(8)
+    v = rng.normal(size=dense.shape[0]) + 1j * rng.normal(size=dense.shape[0])
+    ref = expected_op @ v
+    assert np.linalg.norm(h.matvec(v) - ref) / np.linalg.norm(ref) < 1e-12
+    x = torch.from_numpy(v).to("cuda", torch.complex64)
+    y = torch.empty_like(x)
+    h.apply(x, y, precision=64)
+    assert np.linalg.norm(y.cpu().numpy() - ref) / np.linalg.norm(ref) < 2e-6
