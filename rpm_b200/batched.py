@@ -121,6 +121,21 @@ class BatchedPropagator:
             buf[b, :n].copy_(src.reshape(-1)[:n])
         return buf
 
+    def shape_order(self, system_index):
+        """A stable order that puts trajectories of systems with the same shape
+        (dimensions and radical split) next to each other, or None when they
+        already are.  ``propagate_device`` launches H psi once per run of one
+        shape, on the shape-specialised passes where the shape allows."""
+        keys = {}
+        for h in self.hamiltonians:
+            keys.setdefault((tuple(h.dimensions), tuple(getattr(h, "left_axes", ()))), len(keys))
+        shape = np.array([keys[(tuple(self.hamiltonians[k].dimensions),
+                                tuple(getattr(self.hamiltonians[k], "left_axes", ())))] for k in system_index])
+        runs = 1 + int(np.count_nonzero(np.diff(shape))) if shape.size else 0
+        if runs <= len(np.unique(shape)):
+            return None
+        return np.argsort(shape, kind="stable")
+
     def propagate_device(self, psi, times_us, system_index, *, stream=None):
         """Run on a prepared (trajectories, ld) complex128 CUDA buffer (overwritten
         with the final states).  Returns device tensors (values, state_errors)
@@ -177,8 +192,19 @@ class BatchedPropagator:
         idx = np.zeros(ntraj, dtype=np.int32) if system_index is None else np.asarray(system_index, dtype=np.int32)
         if idx.size != ntraj:
             raise ValueError("system_index must give one system per trajectory")
-        psi = self.load_states(initial_states, idx)
-        values, errs, stats = self.propagate_device(psi, times, idx)
+        # trajectories of one shape run as one launch group: order them by shape
+        order = self.shape_order(idx)
+        states = initial_states if order is None else [initial_states[k] for k in order]
+        run_idx = idx if order is None else idx[order]
+        psi = self.load_states(states, run_idx)
+        values, errs, stats = self.propagate_device(psi, times, run_idx)
+        if order is not None:
+            inverse = np.empty_like(order)
+            inverse[order] = np.arange(order.size)
+            torch = _torch()
+            inv_t = torch.as_tensor(inverse, device=values.device)
+            values, errs, psi = values[inv_t], errs[inv_t], psi[inv_t]
+            stats = [stats[int(k)] for k in inverse]
         yields = None
         rates = self.recombination()
         if rates is not None:

@@ -199,9 +199,9 @@ __global__ void __launch_bounds__(kEwThreads) k_b_start(BatchDev B) {
 
 // v_j <- scale * V_j (in place);  w = V_{j+1} - alpha_j v_j - beta_{j-1} v_{j-1};
 // beta_j = ||w||, scale = 1 / beta_j; breakdown when beta_j is at round-off level.
-__global__ void __launch_bounds__(kEwThreads) k_b_update(BatchDev B, int j) {
+__global__ void __launch_bounds__(kEwThreads) k_b_update(BatchDev B, int j, int b0) {
   __shared__ double red[32];
-  const int b = blockIdx.y;
+  const int b = blockIdx.y + b0;
   TrajState& s = B.st[b];
   if (s.skip) return;
   const float sc = (float)s.scale;
@@ -587,6 +587,23 @@ __global__ void __launch_bounds__(kEwThreads) k_b_arn_dots(BatchDev B, int j, in
       h = pass == 1 ? t : cadd(h, t);
     }
     if (threadIdx.x == 0) B.count[b] = 0;
+  }
+}
+
+// v_j <- scale * V_j in place for trajectories b0 + blockIdx.y (Arnoldi on
+// the general cube kernels; the shape-specialised passes do this while staging).
+__global__ void __launch_bounds__(kEwThreads) k_b_arn_scale(BatchDev B, int j, int b0) {
+  const int b = blockIdx.y + b0;
+  TrajState& s = B.st[b];
+  if (s.skip) return;
+  const float sc = (float)s.scale;
+  float2* v = B.V + (size_t)b * (B.m + 1) * B.ld + (size_t)j * B.ld;
+  const long long end = min(s.n, (long long)(blockIdx.x + 1) * kEwChunk);
+  for (long long i = (long long)blockIdx.x * kEwChunk + threadIdx.x; i < end; i += kEwThreads) {
+    float2 x = v[i];
+    x.x *= sc;
+    x.y *= sc;
+    v[i] = x;
   }
 }
 
@@ -1036,7 +1053,16 @@ struct rpm_batch {
   long long probe_samples = 0;
   long long kernel_launches = 0, replays = 0;
   int launches_per_step = 0;
-  bool fused = false;  // Lanczos recurrence fused into the H psi passes
+  bool fused = false;  // every group runs the fused passes
+  // Consecutive trajectories whose systems share one shape (digit pattern and
+  // layout) form a group; each group's H psi is one launch pair with its own
+  // plan, on the shape-specialised passes when the shape allows.
+  struct ShapeGroup {
+    int b0, nb;
+    rpm::CubePlan plan;
+  };
+  std::vector<ShapeGroup> groups;
+  int dot_stride = 1;  // partial-sum slots per trajectory
 };
 
 namespace rpm {
@@ -1085,6 +1111,32 @@ static Layout layout(const rpm_batch* B, int ntraj, int ntimes, int nblk, int gb
   return L;
 }
 
+// Launch arguments of trajectories b0, b0 + 1, ... (every per-trajectory
+// pointer advanced by b0); `dstride` partial-sum slots per trajectory.
+static HpsiArgs<float2> group_args(const HpsiArgs<float2>& a, int b0, int dstride) {
+  HpsiArgs<float2> c = a;
+  const long long s = b0;
+  c.in += s * a.ld;
+  c.out += s * a.ld;
+  if (c.in_scale) c.in_scale += s * a.scale_stride;
+  if (c.skip) c.skip += s * a.skip_stride;
+  if (c.sys_of) c.sys_of += s;
+  if (c.dot_out) c.dot_out += s * a.dot_stride;
+  if (c.dot_part) c.dot_part += s * dstride;
+  if (c.dot_count) c.dot_count += s;
+  LanczosFuse& z = c.lz;
+  if (z.prev) z.prev += s * a.ld;
+  if (z.alpha_prev) z.alpha_prev += s * z.dstride;
+  if (z.beta_prev) z.beta_prev += s * z.dstride;
+  if (z.alpha_out) z.alpha_out += s * z.dstride;
+  if (z.beta_out) z.beta_out += s * z.dstride;
+  if (z.scale_out) z.scale_out += s * z.dstride;
+  if (z.stop) z.stop += s * z.istride;
+  if (z.skip) z.skip += s * z.istride;
+  if (z.msize) z.msize += s * z.istride;
+  return c;
+}
+
 static void record_step(rpm_batch* Bh, const BatchDev& B, const Layout& L, cudaStream_t st) {
   char* base = static_cast<char*>(Bh->buf);
   const int m = B.m;
@@ -1107,27 +1159,47 @@ static void record_step(rpm_batch* Bh, const BatchDev& B, const Layout& L, cudaS
   cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
   check_cuda(cudaStreamIsCapturing(st, &capturing), "capture status");
   const unsigned probe_flags = capturing == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : 0u;
-  // The shape-specialised passes carry the Lanczos recurrence themselves
-  // (LanczosFuse: no update kernel); otherwise H psi + k_b_update.  Non-
-  // Hermitian systems (unequal recombination rates) run Arnoldi instead.
+  const int D = Bh->dot_stride;
+  // Per shape group: the shape-specialised passes carry the Lanczos
+  // recurrence themselves (LanczosFuse: no update kernel); otherwise H psi on
+  // the general cube kernels + k_b_update.  Non-Hermitian systems (unequal
+  // recombination rates) run Arnoldi instead.
   a.in = B.V;
   a.out = B.V + B.ld;
-  const bool fused = cube_fast_usable(a, Bh->plan, ya);
+  std::vector<char> gfused(Bh->groups.size());
+  bool all_fused = true;
+  for (size_t g = 0; g < Bh->groups.size(); ++g) {
+    const auto& G = Bh->groups[g];
+    gfused[g] = cube_fast_usable(group_args(a, G.b0, D), G.plan, ya + (size_t)G.b0 * B.ld) ? 1 : 0;
+    all_fused = all_fused && gfused[g];
+  }
+  int per_iter = 0;
+  for (size_t g = 0; g < Bh->groups.size(); ++g) per_iter += gfused[g] ? 2 : 3;
   if (B.arnoldi) {
-    if (!fused) fail(RPM_E_UNSUPPORTED, "unequal recombination rates need the shape-specialised H psi passes");
     for (int j = 0; j < m; ++j) {
       a.in = B.V + (size_t)j * B.ld;
       a.out = B.V + (size_t)(j + 1) * B.ld;
       LanczosFuse& z = a.lz;
       z = LanczosFuse{};
-      z.on = 2;
       z.first = j == 0;
       z.last = j == m - 1;
       z.j = j;
       a.dot_out = nullptr;
       a.dot_part = nullptr;
       if (j == probe_j) check_cuda(cudaEventRecordWithFlags(Bh->probe0, st, probe_flags), "probe record");
-      if (!launch_cube_fast(a, Bh->plan, ya, B.ntraj, st)) fail(RPM_E_INVALID, "H psi passes unavailable");
+      for (size_t g = 0; g < Bh->groups.size(); ++g) {
+        const auto& G = Bh->groups[g];
+        HpsiArgs<float2> ak = group_args(a, G.b0, D);
+        float2* yk = ya + (size_t)G.b0 * B.ld;
+        if (gfused[g]) {
+          ak.lz.on = 2;  // pass R scales v_j (written back) while staging
+          if (!launch_cube_fast(ak, G.plan, yk, G.nb, st)) fail(RPM_E_INVALID, "H psi passes unavailable");
+        } else {
+          // one shape per launch: H (scale V_j), then V_j *= scale
+          launch_cube<float2>(ak, G.plan, yk, G.nb, st);
+          k_b_arn_scale<<<dim3(B.nblk, G.nb), kEwThreads, 0, st>>>(B, j, G.b0);
+        }
+      }
       if (j == probe_j) check_cuda(cudaEventRecordWithFlags(Bh->probe1, st, probe_flags), "probe record");
       for (int pass = 1; pass <= 2; ++pass) {
         k_b_arn_dots<<<ew, kEwThreads, 0, st>>>(B, j, pass);
@@ -1135,7 +1207,7 @@ static void record_step(rpm_batch* Bh, const BatchDev& B, const Layout& L, cudaS
       }
     }
     Bh->fused = false;
-    Bh->launches_per_step = 1 + 6 * m + 4;
+    Bh->launches_per_step = 1 + (per_iter + 4) * m + 4;
     check_cuda(cudaEventRecord(Bh->ev_fork, st), "fork record");
     check_cuda(cudaStreamWaitEvent(Bh->side, Bh->ev_fork, 0), "fork wait");
     k_b_gram<<<dim3(B.gblk, B.ntraj), 256, 0, Bh->side>>>(B);
@@ -1152,35 +1224,43 @@ static void record_step(rpm_batch* Bh, const BatchDev& B, const Layout& L, cudaS
     a.out = B.V + (size_t)(j + 1) * B.ld;
     // While capturing, external records become event-record nodes of the graph.
     if (j == probe_j) check_cuda(cudaEventRecordWithFlags(Bh->probe0, st, probe_flags), "probe record");
-    if (fused) {
-      LanczosFuse& z = a.lz;
-      z.on = 1;
-      z.first = j == 0;
-      z.last = j == m - 1;
-      z.j = j;
-      z.prev = j > 0 ? B.V + (size_t)(j - 1) * B.ld : nullptr;
-      z.alpha_prev = j > 0 ? &B.st[0].alpha[j - 1] : nullptr;
-      z.beta_prev = j > 0 ? &B.st[0].beta[j - 1] : nullptr;
-      z.alpha_out = &B.st[0].alpha[j];
-      z.beta_out = &B.st[0].beta[j];
-      z.scale_out = &B.st[0].scale;
-      z.stop = &B.st[0].stop;
-      z.skip = &B.st[0].skip;
-      z.msize = &B.st[0].msize;
-      z.dstride = kStateDoubles;
-      z.istride = kStateInts;
-      z.breakdown_rel = B.breakdown_rel;
-      a.dot_out = nullptr;
-      if (!launch_cube_fast(a, Bh->plan, ya, B.ntraj, st)) fail(RPM_E_INVALID, "fused Lanczos passes unavailable");
-    } else {
-      a.dot_out = &B.st[0].alpha[j];
-      launch_cube<float2>(a, Bh->plan, ya, B.ntraj, st);
+    LanczosFuse& z = a.lz;
+    z = LanczosFuse{};
+    z.on = 1;
+    z.first = j == 0;
+    z.last = j == m - 1;
+    z.j = j;
+    z.prev = j > 0 ? B.V + (size_t)(j - 1) * B.ld : nullptr;
+    z.alpha_prev = j > 0 ? &B.st[0].alpha[j - 1] : nullptr;
+    z.beta_prev = j > 0 ? &B.st[0].beta[j - 1] : nullptr;
+    z.alpha_out = &B.st[0].alpha[j];
+    z.beta_out = &B.st[0].beta[j];
+    z.scale_out = &B.st[0].scale;
+    z.stop = &B.st[0].stop;
+    z.skip = &B.st[0].skip;
+    z.msize = &B.st[0].msize;
+    z.dstride = kStateDoubles;
+    z.istride = kStateInts;
+    z.breakdown_rel = B.breakdown_rel;
+    for (size_t g = 0; g < Bh->groups.size(); ++g) {
+      const auto& G = Bh->groups[g];
+      HpsiArgs<float2> ak = group_args(a, G.b0, D);
+      float2* yk = ya + (size_t)G.b0 * B.ld;
+      if (gfused[g]) {
+        ak.dot_out = nullptr;
+        if (!launch_cube_fast(ak, G.plan, yk, G.nb, st)) fail(RPM_E_INVALID, "fused Lanczos passes unavailable");
+      } else {
+        ak.lz = LanczosFuse{};
+        ak.dot_out = &B.st[G.b0].alpha[j];
+        launch_cube<float2>(ak, G.plan, yk, G.nb, st);
+        k_b_update<<<dim3(B.nblk, G.nb), kEwThreads, 0, st>>>(B, j, G.b0);
+      }
     }
     if (j == probe_j) check_cuda(cudaEventRecordWithFlags(Bh->probe1, st, probe_flags), "probe record");
-    if (!fused) k_b_update<<<ew, kEwThreads, 0, st>>>(B, j);
   }
+  const bool fused = all_fused;
   Bh->fused = fused;
-  Bh->launches_per_step = 1 + (fused ? 2 : 3) * m + 4;
+  Bh->launches_per_step = 1 + per_iter * m + 4;
   const size_t ctl_smem = sizeof(double) * 2 * kRecDoubles;
   check_cuda(cudaEventRecord(Bh->ev_fork, st), "fork record");
   check_cuda(cudaStreamWaitEvent(Bh->side, Bh->ev_fork, 0), "fork wait");
@@ -1211,7 +1291,32 @@ static void run_batch(rpm_batch* Bh, int ntraj, const int* sys_of, void* psi, co
   }
   const int nblk = (int)((Bh->ld + kEwChunk - 1) / kEwChunk);
   const int gblk = std::max(1, std::min(32, (int)((Bh->ld / 4 + kGramChunk - 1) / kGramChunk)));
-  const int dot_blocks = std::max(Bh->plan.nl, 1);  // pass R grid.x <= nl
+  // shape groups: runs of consecutive trajectories whose systems share a shape
+  auto same_shape = [](const rpm_system* x, const rpm_system* y) {
+    if (x == y) return true;
+    if (x->n != y->n || x->nl != y->nl || x->nr != y->nr || x->cube_l.K != y->cube_l.K || x->cube_r.K != y->cube_r.K)
+      return false;
+    for (int k = 0; k < x->cube_l.K; ++k)
+      if (x->cube_l.dim[k] != y->cube_l.dim[k]) return false;
+    for (int k = 0; k < x->cube_r.K; ++k)
+      if (x->cube_r.dim[k] != y->cube_r.dim[k]) return false;
+    return x->offl == y->offl && x->offr == y->offr;
+  };
+  Bh->groups.clear();
+  for (int b = 0; b < ntraj;) {
+    int e = b + 1;
+    while (e < ntraj && same_shape(Bh->systems[sys_of[e]], Bh->systems[sys_of[b]])) ++e;
+    std::vector<rpm_system*> members;
+    for (int k = b; k < e; ++k) {
+      rpm_system* sk = Bh->systems[sys_of[k]];
+      if (std::find(members.begin(), members.end(), sk) == members.end()) members.push_back(sk);
+    }
+    Bh->groups.push_back({b, e - b, cube_plan(members.data(), (int)members.size())});
+    b = e;
+  }
+  // partial-sum slots per trajectory: general pass R (grid.x <= nl) or fused pass L (3 per block)
+  const int dot_blocks = std::max({Bh->plan.nl, 3 * (Bh->plan.half_r / 8), 1});
+  Bh->dot_stride = dot_blocks;
   const Layout L = layout(Bh, ntraj, ntimes, nblk, gblk, dot_blocks);
   if (L.total > Bh->buf_bytes) {
     free_graph(Bh);

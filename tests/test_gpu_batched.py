@@ -98,3 +98,27 @@ def test_batched_rejects_bad_times(rb, golden):
     bp = BatchedPropagator([h], krylov_dimension=16)
     with pytest.raises(ValueError):
         bp.propagate(golden["small_psi0"], [0.2, 0.1])
+
+
+def test_shape_groups_in_caller_order(rb):
+    """propagate_device on an interleaved order (one launch group per run of one shape) gives the
+    same populations as propagate, which orders trajectories by shape first."""
+    import torch
+
+    from rpm_b200 import synthetic
+    from rpm_b200.batched import BatchedPropagator
+
+    full = synthetic.full_system()
+    systems = [synthetic.prefix_system(full, 3), synthetic.prefix_system(full, 5)]
+    hams = [rb.CompiledFullPairHamiltonian(s.dimensions, s.terms(0.5, 0.1), left_axes=s.left_axes,
+                                           right_axes=s.right_axes) for s in systems]
+    assert [h._system.fast_hpsi for h in hams] == [False, True]
+    idx = np.array([1, 0, 1, 0], dtype=np.int32)
+    psi = [synthetic.random_phase_vectors(systems[k].dimensions, 1, 300 + b)[0] for b, k in enumerate(idx)]
+    times = np.arange(81) * 0.00125
+    bp = BatchedPropagator(hams, krylov_dimension=24, state_error_budget=1e-9)
+    sorted_run = bp.propagate(psi, times, system_index=idx)
+    buf = bp.load_states(psi, idx)
+    values, _, _ = bp.propagate_device(buf, times, idx)
+    np.testing.assert_allclose(values.cpu().numpy(), sorted_run.observable_values, atol=2e-6)
+    assert torch.isfinite(buf).all()

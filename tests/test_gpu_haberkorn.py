@@ -144,3 +144,37 @@ def test_non_hermitian_action_on_the_general_cube_kernels():
     y = torch.empty_like(x)
     h.apply(x, y, precision=64)
     assert np.linalg.norm(y.cpu().numpy() - ref) / np.linalg.norm(ref) < 2e-6
+
+
+@pytest.mark.gpu
+def test_uneven_sizes_with_unequal_rates_match_dense_oracle():
+    """Uneven system sizes (96, 768 and 864 dimensions, interleaved) with kS = 1e6, kT = 2e6 s^-1 in one
+    propagate call: one launch group per shape (fused Arnoldi passes for the 768-dimension shape, the
+    general cube kernels for the others)."""
+    import rpm_b200 as rb
+    from rpm_b200 import synthetic
+    from rpm_b200.batched import BatchedPropagator
+
+    systems = [synthetic.small_system(), synthetic.make_system(31, (1, 3), (0, 3)),
+               synthetic.prefix_system(synthetic.full_system(), 3)]
+    rates = (1.0, 2.0)
+    hams, dense = [], []
+    for k, sysm in enumerate(systems):
+        terms = sysm.terms(0.3 + 0.4 * k, 0.2 * k)
+        h = rb.CompiledFullPairHamiltonian(sysm.dimensions, terms, left_axes=sysm.left_axes,
+                                           right_axes=sysm.right_axes)
+        h.set_recombination_rates(*rates)
+        hams.append(h)
+        dense.append(oracle.MatrixFreeHamiltonian(sysm.dimensions, [oracle.LocalTerm(t.axes, t.operator)
+                                                                   for t in terms]).explicit_matrix())
+    assert [h._system.fast_hpsi for h in hams] == [False, True, False]
+    index = [0, 1, 2, 0, 1, 2]
+    states = [synthetic.random_phase_vectors(systems[k].dimensions, 1, 50 + b)[0] for b, k in enumerate(index)]
+    times = np.arange(801) * 0.00125  # 0 .. 1 us
+    bp = BatchedPropagator(hams, krylov_dimension=24, state_error_budget=1e-9)
+    assert bp.shape_order(np.array(index)) is not None
+    out = bp.propagate(states, times, system_index=index)
+    for b, (psi, k) in enumerate(zip(states, index)):
+        factored, y = oracle.haberkorn_dense(dense[k], systems[k].dimensions, psi, times, *rates)
+        assert np.max(np.abs(out.observable_values[b] - factored)) < 1e-5
+        assert abs(out.yields[b] - y) < 1e-6
