@@ -485,6 +485,8 @@ def main() -> None:
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison trajectory")
     p.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-gradient side measurement")
+    p.add_argument("--adjoint-only", action="store_true",
+                   help="diagnostic: only the adjoint side measurement (--vectors trajectories, --horizon us)")
     p.add_argument("--horizon", type=float, default=HORIZON_US,
                    help="propagation horizon in us (5 us is the benchmark workload; shorter only for profiling)")
     p.add_argument("--hpsi-only", type=int, default=0, metavar="K",
@@ -494,6 +496,16 @@ def main() -> None:
         raise SystemExit("steps must be >= 1 and warmup >= 0")
     if args.hpsi_only > 0:
         hpsi_probe(args)
+        return
+    if args.adjoint_only:
+        import torch
+
+        from rpm_b200 import synthetic
+
+        full = synthetic.full_system()
+        out = adjoint_sample(full, synthetic.fibonacci_sphere(args.orientations)[0], torch.device("cuda", 0),
+                             vectors=args.vectors, horizon_us=args.horizon)
+        print(json.dumps(out), flush=True)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
