@@ -131,3 +131,19 @@ def test_synthetic_systems_have_reference_shapes():
         np.testing.assert_allclose(t.operator, t.operator.conj().T, atol=1e-12)
     dirs = synthetic.fibonacci_sphere(12)
     assert len(dirs) == 12 and all(0 <= th <= math.pi for th, _ in dirs)
+
+
+def test_batched_shape_order_groups_trajectories_by_shape():
+    from types import SimpleNamespace
+
+    from rpm_b200.batched import BatchedPropagator
+
+    a = SimpleNamespace(dimensions=(2, 2, 3, 2), left_axes=(0, 2))
+    b = SimpleNamespace(dimensions=(2, 2, 3, 2, 2), left_axes=(0, 2))
+    a2 = SimpleNamespace(dimensions=(2, 2, 3, 2), left_axes=(0, 2))  # same shape as a, another system
+    fake = SimpleNamespace(hamiltonians=[a, b, a2])
+    assert BatchedPropagator.shape_order(fake, np.array([0, 2, 1, 1])) is None  # already one run per shape
+    order = BatchedPropagator.shape_order(fake, np.array([1, 0, 1, 2, 0]))
+    assert list(order) == [1, 3, 4, 0, 2]  # stable; shapes in the order of the Hamiltonian list
+    grouped = np.array([1, 0, 1, 2, 0])[order]
+    assert list(grouped) == [0, 2, 0, 1, 1]
