@@ -9,8 +9,9 @@ graph.  The Krylov basis and H psi are complex64; alpha/beta, the state
 between steps, the tridiagonal exponential, the error control, the singlet
 Gram and populations and the Simpson yield are FP64.
 
-Differences from the reference controller (the batched path is judged on
-yields against the FP64 path): the Krylov dimension is fixed, and instead of
+Differences from the reference controller (the batched path is held to its
+yields against the FP64 path, not to the reference's step decisions): the
+Krylov dimension is fixed, and instead of
 halving rejected steps, the step is the largest one whose embedded error
 estimate meets the budget for that basis -- the basis does not depend on the
 step, so no Krylov work is ever discarded.
