@@ -295,6 +295,53 @@ def adjoint_sample(full, direction, dev, vectors: int = 16, horizon_us: float = 
     return out
 
 
+def uneven_sample(args) -> dict:
+    """Uneven system sizes with unequal recombination rates in one propagate
+    call: equal-count nuclear prefixes of 3, 5 and 7 nuclei per radical (864,
+    13,824 and 221,184 dimensions), kS = 1e6 and kT = 2e6 s^-1, trajectories
+    split 16 : 10 : 6 (the 512 : 320 : 192 proportions at 1/32 scale), field
+    directions from a 64 x 32 (theta, phi) grid, Arnoldi per shape group."""
+    import numpy as np
+    import torch
+
+    import rpm_b200 as rb
+    from rpm_b200 import synthetic
+    from rpm_b200.batched import BatchedPropagator
+
+    full = synthetic.full_system()
+    counts = {3: 16, 5: 10, 7: 6}
+    grid = [(math.pi * (i + 0.5) / 64, 2 * math.pi * j / 32) for i in range(64) for j in range(32)]
+    rng = np.random.default_rng(404)
+    hams, states, index, dims = [], [], [], []
+    for per, count in counts.items():
+        sub = synthetic.prefix_system(full, per) if per < 7 else full
+        for t in range(count):
+            th, ph = grid[int(rng.integers(len(grid)))]
+            h = rb.CompiledFullPairHamiltonian(sub.dimensions, sub.terms(th, ph), left_axes=sub.left_axes,
+                                               right_axes=sub.right_axes)
+            h.set_recombination_rates(1.0, 2.0)
+            index.append(len(hams))
+            hams.append(h)
+            states.append(synthetic.random_phase_vectors(sub.dimensions, 1, 900 + len(states))[0])
+            dims.append(sub.dimension)
+    times = np.arange(int(round(args.horizon / GRID_US)) + 1) * GRID_US
+    bp = BatchedPropagator(hams, krylov_dimension=40, state_error_budget=0.5 * YIELD_TOL)
+    first = [0, counts[3], counts[3] + counts[5]]  # one trajectory of each size
+    bp.propagate([states[k] for k in first], times[:9], system_index=first)  # warm-up
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    out = bp.propagate(states, times, system_index=index)
+    e1.record()
+    torch.cuda.synchronize()
+    seconds = e0.elapsed_time(e1) / 1e3
+    return {"probe": "uneven_sizes_unequal_rates", "trajectories": len(states), "seconds": seconds,
+            "trajectories_per_s": len(states) / seconds, "horizon_us": float(times[-1]),
+            "dimensions": {str(d): dims.count(d) for d in sorted(set(dims))},
+            "yield_range": [float(np.min(out.yields)), float(np.max(out.yields))],
+            "krylov_dim": 40, "rates_per_us": [1.0, 2.0]}
+
+
 def b200_arm(args, rank: int, world: int, dist) -> None:
     import numpy as np
     import torch
@@ -485,6 +532,8 @@ def main() -> None:
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison trajectory")
     p.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-gradient side measurement")
+    p.add_argument("--uneven", action="store_true",
+                   help="diagnostic: uneven sizes (864 / 13,824 / 221,184) with unequal rates, --horizon us")
     p.add_argument("--adjoint-only", action="store_true",
                    help="diagnostic: only the adjoint side measurement (--vectors trajectories, --horizon us)")
     p.add_argument("--horizon", type=float, default=HORIZON_US,
@@ -496,6 +545,9 @@ def main() -> None:
         raise SystemExit("steps must be >= 1 and warmup >= 0")
     if args.hpsi_only > 0:
         hpsi_probe(args)
+        return
+    if args.uneven:
+        print(json.dumps(uneven_sample(args)), flush=True)
         return
     if args.adjoint_only:
         import torch
