@@ -325,7 +325,11 @@ def uneven_sample(args) -> dict:
             states.append(synthetic.random_phase_vectors(sub.dimensions, 1, 900 + len(states))[0])
             dims.append(sub.dimension)
     times = np.arange(int(round(args.horizon / GRID_US)) + 1) * GRID_US
-    bp = BatchedPropagator(hams, krylov_dimension=40, state_error_budget=0.5 * YIELD_TOL)
+    from rpm_b200.autotune import KRYLOV_RANGE, tune
+
+    tuning = tune(hams, states, index, horizon_us=0.25, yield_tolerance=YIELD_TOL, krylov_dimensions=KRYLOV_RANGE,
+                  tiles=(len(states),))
+    bp = BatchedPropagator(hams, krylov_dimension=tuning.krylov_dimension, state_error_budget=0.5 * YIELD_TOL)
     first = [0, counts[3], counts[3] + counts[5]]  # one trajectory of each size
     bp.propagate([states[k] for k in first], times[:9], system_index=first)  # warm-up
     torch.cuda.synchronize()
@@ -339,7 +343,9 @@ def uneven_sample(args) -> dict:
             "trajectories_per_s": len(states) / seconds, "horizon_us": float(times[-1]),
             "dimensions": {str(d): dims.count(d) for d in sorted(set(dims))},
             "yield_range": [float(np.min(out.yields)), float(np.max(out.yields))],
-            "krylov_dim": 40, "rates_per_us": [1.0, 2.0]}
+            "krylov_dim": tuning.krylov_dimension,
+            "autotune": [{k: t[k] for k in ("krylov_dimension", "throughput") if k in t} for t in tuning.trials],
+            "rates_per_us": [1.0, 2.0]}
 
 
 def b200_arm(args, rank: int, world: int, dist) -> None:
