@@ -43,11 +43,13 @@ constexpr size_t kArnCtlSmem = sizeof(double2) * 3 * kBMaxK * kBMaxK;  // Arnold
 struct TrajState {
   double t_now, dt, norm, new_norm2, acc_err, step_err, max_norm_err;
   double min_step, max_step, hint, scale;
+  double wnorm2;  // Arnoldi: |H v_j|^2 before the Gram-Schmidt projection
   double alpha[kBMaxK];
   double beta[kBMaxK];
   long long n, matvecs;
   int cursor, npts, done, stop, skip, msize, steps, sys;
-  int status, pad_;
+  int status;
+  int cgs_done;  // Arnoldi: the first projection kept the norm (no second pass)
 };
 static_assert(sizeof(TrajState) % 8 == 0, "TrajState must be a whole number of doubles");
 static_assert(sizeof(TrajState) % 4 == 0, "TrajState must be a whole number of ints");
@@ -536,15 +538,17 @@ __global__ void __launch_bounds__(128) k_b_control(BatchDev B) {
 // ---------------------------------------------------------------------------
 // Arnoldi (non-Hermitian H: unequal recombination rates)
 // ---------------------------------------------------------------------------
-// Classical Gram-Schmidt, applied twice per iteration, of w = V_(j+1) (H v_j
-// from the passes) against v_0..v_j: projections in FP64 from FP32 products,
-// accumulated into column j of the Hessenberg matrix; the second pass's norm
-// gives H(j+1, j) and the scale of the next basis vector.
+// Classical Gram-Schmidt of w = V_(j+1) (H v_j from the passes) against
+// v_0..v_j: projections in FP64 from FP32 products, accumulated into column j
+// of the Hessenberg matrix.  A second pass runs only when the first lost more
+// than 1 - 1/sqrt(2) of the norm (the Kahan-Parlett / DGKS criterion, "twice
+// is enough"); the last pass's norm gives H(j+1, j) and the next scale.
 __global__ void __launch_bounds__(kEwThreads) k_b_arn_dots(BatchDev B, int j, int pass) {
   __shared__ double2 red[kEwThreads / 32][kBMaxK];
+  __shared__ double rn[kEwThreads / 32];
   const int b = blockIdx.y;
   TrajState& s = B.st[b];
-  if (s.skip) return;
+  if (s.skip || (pass == 2 && s.cgs_done)) return;
   const float2* base = B.V + (size_t)b * (B.m + 1) * B.ld;
   const float2* w = base + (size_t)(j + 1) * B.ld;
   const long long i0 = (long long)blockIdx.x * kEwChunk + threadIdx.x;
@@ -555,6 +559,13 @@ __global__ void __launch_bounds__(kEwThreads) k_b_arn_dots(BatchDev B, int j, in
     wv[k] = e < s.n ? w[e] : make_float2(0.f, 0.f);
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (pass == 1) {  // |w|^2 before the projection (second-pass criterion)
+    double nn = 0.0;
+#pragma unroll
+    for (int k = 0; k < kEwPer; ++k) nn = fma((double)wv[k].x, (double)wv[k].x, fma((double)wv[k].y, (double)wv[k].y, nn));
+    nn = warp_sum(nn);
+    if (lane == 0) rn[warp] = nn;
+  }
   for (int i = 0; i <= j; ++i) {
     const float2* v = base + (size_t)i * B.ld;
     double2 acc = make_double2(0.0, 0.0);
@@ -578,7 +589,17 @@ __global__ void __launch_bounds__(kEwThreads) k_b_arn_dots(BatchDev B, int j, in
     for (int w2 = 0; w2 < kEwThreads / 32; ++w2) t = cadd(t, red[w2][i]);
     part[i] = t;
   }
+  if (pass == 1 && threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w2 = 0; w2 < kEwThreads / 32; ++w2) t += rn[w2];
+    B.part[((size_t)b * B.nblk + blockIdx.x) * 2 + 1] = t;
+  }
   if (traj_last_block(B.count + b)) {
+    if (pass == 1 && threadIdx.x == 0) {
+      double t = 0.0;
+      for (int k = 0; k < (int)gridDim.x; ++k) t += __ldcg(B.part + ((size_t)b * B.nblk + k) * 2 + 1);
+      s.wnorm2 = t;
+    }
     for (int i = threadIdx.x; i <= j; i += blockDim.x) {
       double2 t = make_double2(0.0, 0.0);
       for (int k = 0; k < (int)gridDim.x; ++k) t = cadd(t, __ldcg(B.adots + ((size_t)b * B.nblk + k) * kBMaxK + i));
@@ -612,7 +633,7 @@ __global__ void __launch_bounds__(kEwThreads) k_b_arn_axpy(BatchDev B, int j, in
   __shared__ double red[32];
   const int b = blockIdx.y;
   TrajState& s = B.st[b];
-  if (s.skip) return;
+  if (s.skip || (pass == 2 && s.cgs_done)) return;
   for (int i = threadIdx.x; i <= j; i += blockDim.x) {
     const double2 t = B.hcur[(size_t)b * kBMaxK + i];
     hc[i] = make_float2((float)t.x, (float)t.y);
@@ -628,12 +649,20 @@ __global__ void __launch_bounds__(kEwThreads) k_b_arn_axpy(BatchDev B, int j, in
     w[e] = x;
     nn = fma((double)x.x, (double)x.x, fma((double)x.y, (double)x.y, nn));
   }
-  if (pass != 2) return;
   nn = block_sum(nn, red);
   if (threadIdx.x == 0) B.part[((size_t)b * B.nblk + blockIdx.x) * 2] = nn;
   if (traj_last_block(B.count + b) && threadIdx.x == 0) {
     double tot = 0.0;
     for (int k = 0; k < (int)gridDim.x; ++k) tot += __ldcg(B.part + ((size_t)b * B.nblk + k) * 2);
+    if (pass == 1) {
+      // "twice is enough" (Kahan-Parlett / DGKS): a projection that keeps more
+      // than 1/sqrt(2) of the norm needs no second Gram-Schmidt pass
+      s.cgs_done = tot > 0.5 * s.wnorm2 ? 1 : 0;
+      if (!s.cgs_done) {
+        B.count[b] = 0;
+        return;
+      }
+    }
     const double beta = sqrt(tot);
     B.hess[((size_t)b * (kBMaxK + 1) + j + 1) * kBMaxK + j] = make_double2(beta, 0.0);
     s.scale = beta > 0.0 ? 1.0 / beta : 0.0;
