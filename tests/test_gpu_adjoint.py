@@ -155,3 +155,23 @@ def test_full_size_gradients_match_fp64_central_differences():
     # the hyperfine scale also against differences through the adaptive FP64 Krylov path
     s_fd = oracle.central_difference(lambda s: krylov_fp64_yield(np.concatenate([PARAMS[:4], s])), PARAMS[4:])
     _check(res.gradients[0, 4:], s_fd)
+
+
+def test_full_size_complex64_field_gradients_match_complex128():
+    """221,184 dimensions, two trajectories: the complex64 path's angle and pulse derivatives against the
+    complex128 adjoint (itself within 1e-4 of FP64 central differences above).  |B| (a small derivative
+    here, so its absolute complex64 error is a large fraction of it) and the hyperfine scale (complex64
+    states limit it) are checked loosely."""
+    from rpm_b200 import adjoint, synthetic
+
+    full = synthetic.full_system()
+    model = adjoint.ParametricRadicalPair(full, pulse_start_us=0.2, pulse_duration_us=0.5)
+    times = np.arange(641) * 0.00125
+    psi = list(synthetic.random_phase_vectors(full.dimensions, 2, 31))
+    ref = adjoint.AdjointYieldGradient(model, precision="c128")(PARAMS, psi, times, 1.0)
+    got = adjoint.AdjointYieldGradient(model, precision="c64", state_error_budget=1e-8)(PARAMS, psi, times, 1.0)
+    np.testing.assert_allclose(got.yields, ref.yields, rtol=0, atol=1e-6)
+    for b in range(len(psi)):
+        _check(got.gradients[b, 1:4], ref.gradients[b, 1:4])
+        _check(got.gradients[b, :1], ref.gradients[b, :1], rtol=1e-2)
+        _check(got.gradients[b, 4:], ref.gradients[b, 4:], rtol=3e-2)
