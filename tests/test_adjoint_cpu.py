@@ -131,3 +131,17 @@ def test_dense_oracle_differences_pin_an_exact_derivative():
     exact = oracle.simpson(np.array(pops_d), t)
     assert abs(oracle.central_difference(phi, np.array([0.0]))[0] - exact) < 1e-7 * max(1.0, abs(exact))
     assert abs(oracle.central_difference(phi, np.array([0.0]), richardson=True)[0] - exact) < 1e-10 * max(1.0, abs(exact))
+
+
+def test_pulsed_dense_oracle_agrees_with_the_haberkorn_oracle_without_a_pulse():
+    from rpm_b200 import synthetic
+
+    sysm = synthetic.small_system()
+    terms = sysm.terms(0.4, 0.9)
+    h = oracle.MatrixFreeHamiltonian(sysm.dimensions, [oracle.LocalTerm(t.axes, t.operator) for t in terms]).explicit_matrix()
+    psi = synthetic.random_phase_vectors(sysm.dimensions, 1, 6)[0]
+    times = np.arange(161) * 0.00125
+    pops, y = oracle.pulsed_yield_dense(h, h, sysm.dimensions, psi, times, 0.05, 0.15, 0.5)
+    factored, y_h = oracle.haberkorn_dense(h, sysm.dimensions, psi, times, 2.0, 2.0)
+    np.testing.assert_allclose(pops, factored, atol=1e-11)
+    assert abs(y - y_h) < 1e-12
