@@ -740,10 +740,8 @@ static void cube_r_dispatch(const HpsiArgs<T>& a, const CubePlan& p, const T* ya
 
 template <class T>
 void launch_cube(const HpsiArgs<T>& a, const CubePlan& p, T* ya, int batch, cudaStream_t st) {
-  if constexpr (std::is_same<T, float2>::value) {
-    const bool tuned = g_cube_tuning.ni_l || g_cube_tuning.ni_r || g_cube_tuning.tr || g_cube_tuning.tl;
-    if (!tuned && launch_cube_fast(a, p, ya, batch, st)) return;
-  }
+  const bool tuned = g_cube_tuning.ni_l || g_cube_tuning.ni_r || g_cube_tuning.tr || g_cube_tuning.tl;
+  if (!tuned && launch_cube_fast<T>(a, p, ya, batch, st)) return;
   const int ni_l = g_cube_tuning.ni_l > 0 ? std::min(g_cube_tuning.ni_l, p.ni_l) : p.ni_l;
   const int ni_r = g_cube_tuning.ni_r > 0 ? std::min(g_cube_tuning.ni_r, p.ni_r) : p.ni_r;
   if (ni_l >= 2) {

@@ -73,8 +73,10 @@ CubePlan cube_plan(rpm_system* const* systems, int nsys);
 void fast_plan_add(CubePlan& p, const rpm_system* s, bool first);
 // Launches the specialised passes; false (nothing launched) when the plan or
 // the pointers/strides (16-byte alignment) do not allow them.
-bool launch_cube_fast(const HpsiArgs<float2>& a, const CubePlan& p, float2* ya, int batch, cudaStream_t stream);
-bool cube_fast_usable(const HpsiArgs<float2>& a, const CubePlan& p, const float2* ya);
+template <class T>
+bool launch_cube_fast(const HpsiArgs<T>& a, const CubePlan& p, T* ya, int batch, cudaStream_t stream);
+template <class T>
+bool cube_fast_usable(const HpsiArgs<T>& a, const CubePlan& p, const T* ya);
 // Two passes: pass L into `ya` (batch x ld scratch), pass R into a.out.
 template <class T>
 void launch_cube(const HpsiArgs<T>& a, const CubePlan& p, T* ya, int batch, cudaStream_t stream);

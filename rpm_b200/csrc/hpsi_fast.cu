@@ -1,4 +1,5 @@
-// Shape-specialised complex64 H psi passes for the standard radical layout.
+// Shape-specialised H psi passes (complex64 and complex128) for the standard
+// radical layout.
 //
 // Scope: radical-split systems whose tensor axes are ordered
 // (electron A, electron B, left nuclei..., right nuclei...) -- the order of
@@ -67,11 +68,27 @@ struct Shape {
   static constexpr int NTAB = offD(K);
 };
 
+// Element type: complex64 stages two elements per 16-byte copy and carries
+// the fused Lanczos recurrence; complex128 stages one and runs plain H psi
+// (and holds twice the registers per element, so one CTA per SM is assumed).
+template <class T> struct FastT;
+template <> struct FastT<float2> {
+  using R = float;
+  static constexpr int EPU = 2;
+  static constexpr int MINB = 2;
+};
+template <> struct FastT<double2> {
+  using R = double;
+  static constexpr int EPU = 1;
+  static constexpr int MINB = 1;
+};
+
 // Per outer index: diagonal and electron-flip coefficients merged over the
 // electron-only term and every outer digit.
+template <class T>
 struct ORec {
-  float d[2];
-  float2 f[2];
+  typename FastT<T>::R d[2];
+  T f[2];
 };
 
 constexpr int align16c(int bytes) { return (bytes + 15) & ~15; }
@@ -82,22 +99,26 @@ __device__ __forceinline__ void copy16(void* smem_dst, const void* gmem_src) {
 }
 __device__ __forceinline__ void copy_wait_all() { asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory"); }
 
-__device__ __forceinline__ float2 rmacf(float d, float2 x, float2 acc) {
-  acc.x = fmaf(d, x.x, acc.x);
-  acc.y = fmaf(d, x.y, acc.y);
+template <class T>
+__device__ __forceinline__ T rmac(typename FastT<T>::R d, T x, T acc) {
+  acc.x = fma(d, x.x, acc.x);
+  acc.y = fma(d, x.y, acc.y);
   return acc;
 }
 
-__device__ __forceinline__ bool skip_vec(const HpsiArgs<float2>& a, int b) {
+template <class T>
+__device__ __forceinline__ bool skip_vec(const HpsiArgs<T>& a, int b) {
   return a.skip && a.skip[(long long)b * a.skip_stride] != 0;
 }
-__device__ __forceinline__ double in_scale(const HpsiArgs<float2>& a, int b) {
+template <class T>
+__device__ __forceinline__ double in_scale(const HpsiArgs<T>& a, int b) {
   return a.in_scale ? a.in_scale[(long long)b * a.scale_stride] : 1.0;
 }
 
 // Fused <in_scaled, H in_scaled>: per-block partial; the last block of
 // vector b sums the partials in block order (deterministic).
-__device__ void finish_dot_fast(const HpsiArgs<float2>& a, int b, double mine) {
+template <class T>
+__device__ void finish_dot_fast(const HpsiArgs<T>& a, int b, double mine) {
   __shared__ double red[32];
   __shared__ bool last;
 #pragma unroll
@@ -182,8 +203,8 @@ __device__ void finish_lanczos(const HpsiArgs<float2>& a, int b, double s0, doub
 
 // Merged diagonal / flip coefficients of the two register-cube digits
 // (digits K-2 -> bit 1 of i, K-1 -> bit 0 of i).
-template <class S>
-__device__ __forceinline__ void cube_consts(const float2* tab, float (&din)[2][4], float2 (&fin)[2][4]) {
+template <class S, class T>
+__device__ __forceinline__ void cube_consts(const T* tab, typename FastT<T>::R (&din)[2][4], T (&fin)[2][4]) {
   constexpr int K = S::K;
 #pragma unroll
   for (int e = 0; e < 2; ++e)
@@ -195,12 +216,12 @@ __device__ __forceinline__ void cube_consts(const float2* tab, float (&din)[2][4
 }
 
 // Register-cube transitions of the two cube digits.
-template <class S>
-__device__ __forceinline__ void cube_inner(const float2* tab, const float2 (&x)[2][4], float2 (&acc)[2][4]) {
+template <class S, class T>
+__device__ __forceinline__ void cube_inner(const T* tab, const T (&x)[2][4], T (&acc)[2][4]) {
   constexpr int K = S::K;
 #pragma unroll
   for (int q = 0; q < 2; ++q) {
-    const float2* X = tab + S::offX(K - 2 + q);
+    const T* X = tab + S::offX(K - 2 + q);
     const int sh = 1 - q;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
@@ -216,7 +237,8 @@ __device__ __forceinline__ void cube_inner(const float2* tab, const float2 (&x)[
 }
 
 // acc[e][i] += c[e][ep] * y[ep][i]
-__device__ __forceinline__ void partner_mac(const float2 (&c)[2][2], const float2 (&y)[2][4], float2 (&acc)[2][4]) {
+template <class T>
+__device__ __forceinline__ void partner_mac(const T (&c)[2][2], const T (&y)[2][4], T (&acc)[2][4]) {
 #pragma unroll
   for (int ep = 0; ep < 2; ++ep)
 #pragma unroll
@@ -228,9 +250,9 @@ __device__ __forceinline__ void partner_mac(const float2 (&c)[2][2], const float
 
 // Coefficients of one partner along outer digit k (value m -> mp) for every
 // (output electron e, input electron ep).
-template <class S>
-__device__ __forceinline__ void outer_coefs(const float2* tab, int k, int m, int mp, float2 (&c)[2][2]) {
-  const float2* X = tab + S::offX(k);
+template <class S, class T>
+__device__ __forceinline__ void outer_coefs(const T* tab, int k, int m, int mp, T (&c)[2][2]) {
+  const T* X = tab + S::offX(k);
   const int d = S::dim(k);
 #pragma unroll
   for (int e = 0; e < 2; ++e)
@@ -242,46 +264,49 @@ __device__ __forceinline__ void outer_coefs(const float2* tab, int k, int m, int
 // Pass R: 16 rows (eA, l) x all (eB, r) per CTA; lane bits 0-3 = row, lane
 // bit 4 selects one of two outer indices of the warp's task.
 // ---------------------------------------------------------------------------
-template <int N1, int NH>
+template <class T, int N1, int NH>
 struct PassR {
   using S = Shape<N1, NH>;
+  static constexpr int EPU = FastT<T>::EPU;
   static constexpr int TR = 16;          // rows per CTA
   static constexpr int HR = S::HALF;
   static constexpr int NO = HR / 4;      // outer indices per row
   static constexpr int NTASK = (NO + 1) / 2;  // warp tasks: two outer indices each
-  static constexpr int RS = 2 * HR + 2;  // padded row stride (elements): an odd number of 16-byte units
-  static constexpr int TAB_BYTES = align16c(S::NTAB * 8);
-  static constexpr int OREC_BYTES = align16c(NO * (int)sizeof(ORec));
-  // tables, records, the tile and (fused Lanczos) the tile of v_{j-1}
-  static constexpr int SMEM = TAB_BYTES + OREC_BYTES + 2 * TR * RS * 8;
+  // padded row stride (elements): an odd number of 16-byte units
+  static constexpr int RS = EPU == 2 ? 2 * HR + 2 : 2 * HR + 1;
+  static constexpr int TAB_BYTES = align16c(S::NTAB * (int)sizeof(T));
+  static constexpr int OREC_BYTES = align16c(NO * (int)sizeof(ORec<T>));
+  // tables, records, the tile and (complex64, fused Lanczos) the tile of v_{j-1}
+  static constexpr int SMEM = TAB_BYTES + OREC_BYTES + (EPU == 2 ? 2 : 1) * TR * RS * (int)sizeof(T);
   // 8 warps: measured faster than 12 or 16, which force register spills
   static constexpr int WARPS =
       NTASK % 8 == 0 ? 8 : NTASK % 6 == 0 ? 6 : NTASK % 4 == 0 ? 4 : NTASK % 3 == 0 ? 3 : NTASK < 8 ? NTASK : 8;
   static_assert(NH >= 2, "pass R needs two trailing spin-1/2 digits");
 };
 
-template <int N1, int NH>
-__global__ void __launch_bounds__(PassR<N1, NH>::WARPS * 32, 2)
-    fast_pass_r(HpsiArgs<float2> a, float2* __restrict__ yb) {
-  using P = PassR<N1, NH>;
+template <class T, int N1, int NH>
+__global__ void __launch_bounds__(PassR<T, N1, NH>::WARPS * 32, FastT<T>::MINB)
+    fast_pass_r(HpsiArgs<T> a, T* __restrict__ yb) {
+  using P = PassR<T, N1, NH>;
   using S = typename P::S;
+  using R = typename FastT<T>::R;
   constexpr int K = S::K;
-  constexpr int TR = P::TR, HR = P::HR, NO = P::NO, RS = P::RS;
+  constexpr int TR = P::TR, HR = P::HR, NO = P::NO, RS = P::RS, EPU = P::EPU;
   constexpr int NT = P::WARPS * 32;
   const int b = blockIdx.y;
   if (skip_vec(a, b)) return;
-  const CubeView<float2>* view = a.views + (a.sys_of ? a.sys_of[b] : 0);
+  const CubeView<T>* view = a.views + (a.sys_of ? a.sys_of[b] : 0);
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* tab = reinterpret_cast<float2*>(smem_raw);
-  ORec* orec = reinterpret_cast<ORec*>(smem_raw + P::TAB_BYTES);
-  float2* tile = reinterpret_cast<float2*>(smem_raw + P::TAB_BYTES + P::OREC_BYTES);
-  float2* ptile = tile + TR * RS;
+  T* tab = reinterpret_cast<T*>(smem_raw);
+  ORec<T>* orec = reinterpret_cast<ORec<T>*>(smem_raw + P::TAB_BYTES);
+  T* tile = reinterpret_cast<T*>(smem_raw + P::TAB_BYTES + P::OREC_BYTES);
+  T* ptile = tile + TR * RS;  // complex64 only
   const int half_l = view->half_l;
   const int row0 = blockIdx.x * TR;
   const int rows = min(TR, 2 * half_l - row0);
   const long long quarter = (long long)half_l * HR;
-  const float2* x_in = a.in + (long long)b * a.ld;
-  constexpr int CH = HR / 2;  // 16-byte chunks per half row
+  const T* x_in = a.in + (long long)b * a.ld;
+  constexpr int CH = HR / EPU;  // 16-byte chunks per half row
   const int units = rows * 2 * CH;
   auto unit_at = [&](int idx, int& slot, long long& g) {
     const int rr = idx / (2 * CH), rem = idx - rr * (2 * CH);
@@ -289,14 +314,15 @@ __global__ void __launch_bounds__(PassR<N1, NH>::WARPS * 32, 2)
     const int rho = row0 + rr;
     const int ea = rho >= half_l ? 1 : 0;
     const int llo = rho - ea * half_l;
-    slot = rr * RS + e * HR + 2 * c;
-    g = (2 * ea + e) * quarter + (long long)llo * HR + 2 * c;
+    slot = rr * RS + e * HR + EPU * c;
+    g = (2 * ea + e) * quarter + (long long)llo * HR + EPU * c;
   };
   // fused Lanczos (j > 0): the tile receives w'_j and ptile v_{j-1}; below,
   // v_j = (w'_j - alpha_{j-1} v_{j-1}) * scale replaces w'_j in the tile and in `in`
-  const bool combine = a.lz.on && !a.lz.first;
+  const bool combine = EPU == 2 && a.lz.on && !a.lz.first;
   const bool with_prev = combine && a.lz.on == 1;  // Arnoldi (on == 2) only rescales
-  const float2* pv = with_prev ? a.lz.prev + (long long)b * a.ld : nullptr;
+  const T* pv = nullptr;
+  if constexpr (EPU == 2) pv = with_prev ? a.lz.prev + (long long)b * a.ld : nullptr;
   for (int idx = threadIdx.x; idx < units; idx += NT) {
     int slot;
     long long g;
@@ -307,7 +333,7 @@ __global__ void __launch_bounds__(PassR<N1, NH>::WARPS * 32, 2)
   for (int k = threadIdx.x; k < S::NTAB; k += NT) tab[k] = view->tabR[k];
   __syncthreads();
   for (int o = threadIdx.x; o < NO; o += NT) {
-    ORec r;
+    ORec<T> r;
     r.d[0] = tab[0].x;
     r.d[1] = tab[1].x;
     r.f[0] = tab[2];
@@ -324,11 +350,11 @@ __global__ void __launch_bounds__(PassR<N1, NH>::WARPS * 32, 2)
     orec[o] = r;
   }
   copy_wait_all();
-  if (combine) {
+  if constexpr (EPU == 2) if (combine) {
     // each thread combines the units it copied (visible to it after its own wait)
     const float al = with_prev ? (float)a.lz.alpha_prev[(long long)b * a.lz.dstride] : 0.0f;
     const float sc = (float)in_scale(a, b);
-    float2* xo = const_cast<float2*>(x_in);
+    T* xo = const_cast<T*>(x_in);
     for (int idx = threadIdx.x; idx < units; idx += NT) {
       int slot;
       long long g;
@@ -348,40 +374,45 @@ __global__ void __launch_bounds__(PassR<N1, NH>::WARPS * 32, 2)
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int row = lane & 15, hsel = lane >> 4;
-  const float sf = a.lz.on ? 1.0f : (float)in_scale(a, b);  // fused: the staged v_j is already scaled
+  const R sf = a.lz.on ? R(1) : (R)in_scale(a, b);  // fused: the staged v_j is already scaled
   // Paige's -beta_{j-1} v_{j-1} joins the partial here, where v_{j-1} is staged
-  const float bprev = with_prev ? (float)a.lz.beta_prev[(long long)b * a.lz.dstride] : 0.0f;
-  const float2* rowp = tile + row * RS;
-  const float2* prowp = ptile + row * RS;
-  float din[2][4];
-  float2 fin[2][4];
+  const R bprev = with_prev ? (R)a.lz.beta_prev[(long long)b * a.lz.dstride] : R(0);
+  const T* rowp = tile + row * RS;
+  const T* prowp = ptile + row * RS;
+  R din[2][4];
+  T fin[2][4];
   cube_consts<S>(tab, din, fin);
   const int rho = row0 + row;
   const int ea = rho >= half_l ? 1 : 0;
   const long long gbase = 2 * ea * quarter + (long long)(rho - ea * half_l) * HR;
-  float2* y_b = yb + (long long)b * (a.ya_ld ? a.ya_ld : a.ld) + gbase;
+  T* y_b = yb + (long long)b * (a.ya_ld ? a.ya_ld : a.ld) + gbase;
   for (int t = warp; t < P::NTASK; t += P::WARPS) {
     const int o = min(2 * t + hsel, NO - 1);  // (odd NO: the spare half repeats the last index, no store)
     const bool active = 2 * t + hsel < NO && row < rows;
-    const ORec rec = orec[o];
-    auto load = [&](int delta, float2 (&y)[2][4]) {
+    const ORec<T> rec = orec[o];
+    auto load = [&](int delta, T (&y)[2][4]) {
 #pragma unroll
       for (int ep = 0; ep < 2; ++ep) {
-        const float4 u = *reinterpret_cast<const float4*>(rowp + ep * HR + 4 * o + delta);
-        const float4 v = *reinterpret_cast<const float4*>(rowp + ep * HR + 4 * o + delta + 2);
-        y[ep][0] = make_float2(u.x, u.y);
-        y[ep][1] = make_float2(u.z, u.w);
-        y[ep][2] = make_float2(v.x, v.y);
-        y[ep][3] = make_float2(v.z, v.w);
+        if constexpr (EPU == 2) {
+          const float4 u = *reinterpret_cast<const float4*>(rowp + ep * HR + 4 * o + delta);
+          const float4 v = *reinterpret_cast<const float4*>(rowp + ep * HR + 4 * o + delta + 2);
+          y[ep][0] = make_float2(u.x, u.y);
+          y[ep][1] = make_float2(u.z, u.w);
+          y[ep][2] = make_float2(v.x, v.y);
+          y[ep][3] = make_float2(v.z, v.w);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 4; ++i) y[ep][i] = rowp[ep * HR + 4 * o + delta + i];
+        }
       }
     };
-    float2 x[2][4], acc[2][4];
+    T x[2][4], acc[2][4];
     load(0, x);
 #pragma unroll
     for (int e = 0; e < 2; ++e)
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        acc[e][i] = rmacf(rec.d[e] + din[e][i], x[e][i], make_float2(0.f, 0.f));
+        acc[e][i] = rmac<T>(rec.d[e] + din[e][i], x[e][i], czero<T>());
         acc[e][i] = cfma(cadd(rec.f[e], fin[e][i]), x[1 - e][i], acc[e][i]);
       }
     cube_inner<S>(tab, x, acc);
@@ -391,13 +422,24 @@ __global__ void __launch_bounds__(PassR<N1, NH>::WARPS * 32, 2)
 #pragma unroll
       for (int tt = 1; tt < S::dim(k); ++tt) {
         const int mp = m + tt >= S::dim(k) ? m + tt - S::dim(k) : m + tt;
-        float2 c[2][2], y[2][4];
+        T c[2][2], y[2][4];
         outer_coefs<S>(tab, k, m, mp, c);
         load((mp - m) * S::gs(k), y);
         partner_mac(c, y, acc);
       }
     }
-    if (active) {
+    if (active && EPU == 1) {
+#pragma unroll
+      for (int e = 0; e < 2; ++e)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          T v = acc[e][i];
+          v.x *= sf;
+          v.y *= sf;
+          y_b[e * quarter + 4 * o + i] = v;
+        }
+    }
+    if constexpr (EPU == 2) if (active) {
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const long long at = e * quarter + 4 * o;
@@ -433,49 +475,52 @@ __global__ void __launch_bounds__(PassR<N1, NH>::WARPS * 32, 2)
 // Pass L: every l x 16 columns (eB x 8 consecutive r) per CTA; lane bits 0-2
 // = r, bit 3 = eB, bit 4 = digit K-3 of l.  Cube = eA x digits K-2, K-1.
 // ---------------------------------------------------------------------------
-template <int N1, int NH>
+template <class T, int N1, int NH>
 struct PassL {
   using S = Shape<N1, NH>;
+  static constexpr int EPU = FastT<T>::EPU;
   static constexpr int HL = S::HALF;
   static constexpr int NO = HL / 8;  // outer indices
   static constexpr int NL = 2 * HL;
-  static constexpr int TAB_BYTES = align16c(S::NTAB * 8);
-  static constexpr int OREC_BYTES = align16c(NO * (int)sizeof(ORec));
-  static constexpr int SMEM = TAB_BYTES + OREC_BYTES + NL * 16 * 8;
+  static constexpr int TAB_BYTES = align16c(S::NTAB * (int)sizeof(T));
+  static constexpr int OREC_BYTES = align16c(NO * (int)sizeof(ORec<T>));
+  static constexpr int SMEM = TAB_BYTES + OREC_BYTES + NL * 16 * (int)sizeof(T);
   static constexpr int WARPS =
       NO % 8 == 0 ? 8 : NO % 6 == 0 ? 6 : NO % 9 == 0 ? 9 : NO % 4 == 0 ? 4 : NO % 3 == 0 ? 3 : NO < 8 ? NO : 8;
   static_assert(NH >= 3, "pass L needs three trailing spin-1/2 digits");
 };
 
-template <int N1, int NH>
-__global__ void __launch_bounds__(PassL<N1, NH>::WARPS * 32, 2)
-    fast_pass_l(HpsiArgs<float2> a, const float2* __restrict__ yb) {
-  using P = PassL<N1, NH>;
+template <class T, int N1, int NH>
+__global__ void __launch_bounds__(PassL<T, N1, NH>::WARPS * 32, FastT<T>::MINB)
+    fast_pass_l(HpsiArgs<T> a, const T* __restrict__ yb) {
+  using P = PassL<T, N1, NH>;
   using S = typename P::S;
+  using R = typename FastT<T>::R;
   constexpr int K = S::K;
-  constexpr int HL = P::HL, NO = P::NO, NL = P::NL;
+  constexpr int HL = P::HL, NO = P::NO, NL = P::NL, EPU = P::EPU;
   constexpr int NT = P::WARPS * 32;
+  constexpr int UH = 8 / EPU;  // 16-byte units per (l, electron B) row of 8 columns
   const int b = gridDim.y - 1 - blockIdx.y;
   if (skip_vec(a, b)) return;
-  const CubeView<float2>* view = a.views + (a.sys_of ? a.sys_of[b] : 0);
+  const CubeView<T>* view = a.views + (a.sys_of ? a.sys_of[b] : 0);
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* tab = reinterpret_cast<float2*>(smem_raw);
-  ORec* orec = reinterpret_cast<ORec*>(smem_raw + P::TAB_BYTES);
-  float2* tile = reinterpret_cast<float2*>(smem_raw + P::TAB_BYTES + P::OREC_BYTES);
+  T* tab = reinterpret_cast<T*>(smem_raw);
+  ORec<T>* orec = reinterpret_cast<ORec<T>*>(smem_raw + P::TAB_BYTES);
+  T* tile = reinterpret_cast<T*>(smem_raw + P::TAB_BYTES + P::OREC_BYTES);
   const int HR = view->half_r;
   const long long quarter = (long long)HL * HR;
   const int c0 = blockIdx.x * 8;
-  const float2* x_in = a.in + (long long)b * a.ld;
-  for (int idx = threadIdx.x; idx < NL * 8; idx += NT) {
-    const int l = idx >> 3, h = (idx >> 2) & 1, q = idx & 3;
+  const T* x_in = a.in + (long long)b * a.ld;
+  for (int idx = threadIdx.x; idx < NL * 2 * UH; idx += NT) {
+    const int l = idx / (2 * UH), h = (idx / UH) & 1, q = idx % UH;
     const int ea = l >= HL ? 1 : 0;
     const int llo = l - ea * HL;
-    copy16(tile + l * 16 + h * 8 + 2 * q, x_in + (2 * ea + h) * quarter + (long long)llo * HR + c0 + 2 * q);
+    copy16(tile + l * 16 + h * 8 + EPU * q, x_in + (2 * ea + h) * quarter + (long long)llo * HR + c0 + EPU * q);
   }
   for (int k = threadIdx.x; k < S::NTAB; k += NT) tab[k] = view->tabL[k];
   __syncthreads();
   for (int o = threadIdx.x; o < NO; o += NT) {
-    ORec r;
+    ORec<T> r;
     r.d[0] = tab[0].x;
     r.d[1] = tab[1].x;
     r.f[0] = tab[2];
@@ -496,12 +541,12 @@ __global__ void __launch_bounds__(PassL<N1, NH>::WARPS * 32, 2)
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int j = lane & 7, h = (lane >> 3) & 1, lg = lane >> 4, c = lane & 15;
-  const bool fused = a.lz.on == 1;
+  const bool fused = EPU == 2 && a.lz.on == 1;
   const bool store = !fused || !a.lz.last;
-  const float sf = a.lz.on ? 1.0f : (float)in_scale(a, b);  // fused / Arnoldi: pass R wrote the scaled v_j
+  const R sf = a.lz.on ? R(1) : (R)in_scale(a, b);  // fused / Arnoldi: pass R wrote the scaled v_j
   // electron-pair operator rows of (e, h): eB-diagonal part merged, eB flip via the partner column
-  float dp[2];
-  float2 fp[2], pp[2][2];
+  R dp[2];
+  T fp[2], pp[2][2];
 #pragma unroll
   for (int e = 0; e < 2; ++e) {
     dp[e] = view->pair[(e * 2 + h) * 4 + e * 2 + h].x;
@@ -510,8 +555,8 @@ __global__ void __launch_bounds__(PassL<N1, NH>::WARPS * 32, 2)
     for (int ep = 0; ep < 2; ++ep) pp[e][ep] = view->pair[(e * 2 + h) * 4 + ep * 2 + (1 - h)];
   }
   // lane digit K-3
-  float dL[2];
-  float2 fL[2], cL[2][2];
+  R dL[2];
+  T fL[2], cL[2][2];
 #pragma unroll
   for (int e = 0; e < 2; ++e) {
     dL[e] = tab[S::offD(K - 3) + e * 2 + lg].x + dp[e];
@@ -519,30 +564,30 @@ __global__ void __launch_bounds__(PassL<N1, NH>::WARPS * 32, 2)
 #pragma unroll
     for (int ep = 0; ep < 2; ++ep) cL[e][ep] = tab[S::offX(K - 3) + (e * 2 + lg) * 4 + ep * 2 + (1 - lg)];
   }
-  float din[2][4];
-  float2 fin[2][4];
+  R din[2][4];
+  T fin[2][4];
   cube_consts<S>(tab, din, fin);
   // imaginary diagonal of the pair operator: nonzero only with unequal
   // recombination rates (the non-Hermitian -(i/2) |kS - kT| Q term)
-  const bool cdiag = view->pair[0].y != 0.f || view->pair[5].y != 0.f || view->pair[10].y != 0.f ||
-                     view->pair[15].y != 0.f;
-  float gim[2];
+  const bool cdiag = view->pair[0].y != R(0) || view->pair[5].y != R(0) || view->pair[10].y != R(0) ||
+                     view->pair[15].y != R(0);
+  R gim[2];
 #pragma unroll
   for (int e = 0; e < 2; ++e) gim[e] = view->pair[(e * 2 + h) * 4 + e * 2 + h].y;
-  const float2* col = tile + c;
+  const T* col = tile + c;
   const long long cofs = h * quarter + c0 + j;
-  const float2* y_b = yb + (long long)b * (a.ya_ld ? a.ya_ld : a.ld) + cofs;
-  float2* y_out = a.out + (long long)b * a.ld + cofs;
+  const T* y_b = yb + (long long)b * (a.ya_ld ? a.ya_ld : a.ld) + cofs;
+  T* y_out = a.out + (long long)b * a.ld + cofs;
   double dot = 0.0, nw = 0.0, nv = 0.0;
   for (int o = warp; o < NO; o += P::WARPS) {
-    const ORec rec = orec[o];
+    const ORec<T> rec = orec[o];
     const int lo = o * 8 + lg * 4;  // l of cube element i = 0
-    float2 pb[2][4];  // pass-R partial of the cube (with -beta_{j-1} v_{j-1} when fused), loaded early
+    T pb[2][4];  // pass-R partial of the cube (with -beta_{j-1} v_{j-1} when fused), loaded early
 #pragma unroll
     for (int e = 0; e < 2; ++e)
 #pragma unroll
       for (int i = 0; i < 4; ++i) pb[e][i] = __ldcg(y_b + 2 * e * quarter + (long long)(lo + i) * HR);
-    float2 x[2][4], acc[2][4];
+    T x[2][4], acc[2][4];
 #pragma unroll
     for (int e = 0; e < 2; ++e)
 #pragma unroll
@@ -551,13 +596,13 @@ __global__ void __launch_bounds__(PassL<N1, NH>::WARPS * 32, 2)
     for (int e = 0; e < 2; ++e)
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        acc[e][i] = rmacf(rec.d[e] + dL[e] + din[e][i], x[e][i], make_float2(0.f, 0.f));
+        acc[e][i] = rmac<T>(rec.d[e] + dL[e] + din[e][i], x[e][i], czero<T>());
         acc[e][i] = cfma(cadd(cadd(rec.f[e], fL[e]), fin[e][i]), x[1 - e][i], acc[e][i]);
-        if (cdiag) acc[e][i] = cfma(make_float2(0.f, gim[e]), x[e][i], acc[e][i]);
+        if (cdiag) acc[e][i] = cfma(cmake(R(0), gim[e]), x[e][i], acc[e][i]);
       }
     cube_inner<S>(tab, x, acc);
-    auto partner = [&](int delta, int dcol, const float2 (&cc)[2][2]) {
-      float2 y[2][4];
+    auto partner = [&](int delta, int dcol, const T (&cc)[2][2]) {
+      T y[2][4];
 #pragma unroll
       for (int ep = 0; ep < 2; ++ep)
 #pragma unroll
@@ -572,30 +617,34 @@ __global__ void __launch_bounds__(PassL<N1, NH>::WARPS * 32, 2)
 #pragma unroll
       for (int t = 1; t < S::dim(k); ++t) {
         const int mp = m + t >= S::dim(k) ? m + t - S::dim(k) : m + t;
-        float2 cc[2][2];
+        T cc[2][2];
         outer_coefs<S>(tab, k, m, mp, cc);
         partner((mp - m) * S::gs(k), c, cc);
       }
     }
-    float part = 0.f, pw = 0.f, px = 0.f;
+    R part = 0, pw = 0, px = 0;
 #pragma unroll
     for (int e = 0; e < 2; ++e)
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        float2 v;
-        v.x = fmaf(sf, acc[e][i].x, pb[e][i].x);
-        v.y = fmaf(sf, acc[e][i].y, pb[e][i].y);  // fused: w' = H v_j - beta_{j-1} v_{j-1}
+        T v;
+        v.x = fma(sf, acc[e][i].x, pb[e][i].x);
+        v.y = fma(sf, acc[e][i].y, pb[e][i].y);  // fused: w' = H v_j - beta_{j-1} v_{j-1}
         if (store) y_out[2 * e * quarter + (long long)(lo + i) * HR] = v;
-        part = fmaf(x[e][i].x, v.x, fmaf(x[e][i].y, v.y, part));
-        pw = fmaf(v.x, v.x, fmaf(v.y, v.y, pw));
-        px = fmaf(x[e][i].x, x[e][i].x, fmaf(x[e][i].y, x[e][i].y, px));
+        part = fma(x[e][i].x, v.x, fma(x[e][i].y, v.y, part));
+        pw = fma(v.x, v.x, fma(v.y, v.y, pw));
+        px = fma(x[e][i].x, x[e][i].x, fma(x[e][i].y, x[e][i].y, px));
       }
     dot += (double)part * (double)sf;
     nw += (double)pw;
     nv += (double)px;
   }
-  if (fused) finish_lanczos(a, b, dot, nw, nv);
-  else if (a.dot_part && !a.lz.on) finish_dot_fast(a, b, dot);
+  if constexpr (EPU == 2) {
+    if (fused) finish_lanczos(a, b, dot, nw, nv);
+    else if (a.dot_part && !a.lz.on) finish_dot_fast(a, b, dot);
+  } else {
+    if (a.dot_part) finish_dot_fast(a, b, dot);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -615,48 +664,65 @@ void set_smem(K kern, int bytes) {
   done.emplace_back(key, dev);
 }
 
-template <int N1, int NH>
-void launch_l(const HpsiArgs<float2>& a, const float2* yb, int half_r, int batch, cudaStream_t st) {
-  using P = PassL<N1, NH>;
-  auto kern = fast_pass_l<N1, NH>;
+template <class T, int N1, int NH>
+void launch_l(const HpsiArgs<T>& a, const T* yb, int half_r, int batch, cudaStream_t st) {
+  using P = PassL<T, N1, NH>;
+  auto kern = fast_pass_l<T, N1, NH>;
   set_smem(kern, P::SMEM);
   kern<<<dim3(half_r / 8, batch), P::WARPS * 32, P::SMEM, st>>>(a, yb);
   check_launch("fast_pass_l");
 }
 
-template <int N1, int NH>
-void launch_r(const HpsiArgs<float2>& a, float2* yb, int half_l, int batch, cudaStream_t st) {
-  using P = PassR<N1, NH>;
-  auto kern = fast_pass_r<N1, NH>;
+template <class T, int N1, int NH>
+void launch_r(const HpsiArgs<T>& a, T* yb, int half_l, int batch, cudaStream_t st) {
+  using P = PassR<T, N1, NH>;
+  auto kern = fast_pass_r<T, N1, NH>;
   set_smem(kern, P::SMEM);
   kern<<<dim3((2 * half_l + P::TR - 1) / P::TR, batch), P::WARPS * 32, P::SMEM, st>>>(a, yb);
   check_launch("fast_pass_r");
 }
 
-using LaunchL = void (*)(const HpsiArgs<float2>&, const float2*, int, int, cudaStream_t);
-using LaunchR = void (*)(const HpsiArgs<float2>&, float2*, int, int, cudaStream_t);
+template <class T>
+using LaunchL = void (*)(const HpsiArgs<T>&, const T*, int, int, cudaStream_t);
+template <class T>
+using LaunchR = void (*)(const HpsiArgs<T>&, T*, int, int, cudaStream_t);
+
+// Shared memory a CTA may use (the complex128 tiles are twice as large: a
+// pattern whose pass does not fit has no complex128 variant).
+constexpr int kFastMaxSmem = 227 * 1024;
+
+template <class T, int N1, int NH>
+LaunchL<T> fit_l() {
+  return PassL<T, N1, NH>::SMEM <= kFastMaxSmem ? launch_l<T, N1, NH> : nullptr;
+}
+template <class T, int N1, int NH>
+LaunchR<T> fit_r() {
+  return PassR<T, N1, NH>::SMEM <= kFastMaxSmem ? launch_r<T, N1, NH> : nullptr;
+}
 
 // Instantiated digit patterns (spin-1 count, spin-1/2 count) per radical.
-LaunchL pick_l(int n1, int nh) {
-  if (n1 == 2 && nh == 5) return launch_l<2, 5>;
-  if (n1 == 2 && nh == 3) return launch_l<2, 3>;
-  if (n1 == 2 && nh == 4) return launch_l<2, 4>;
-  if (n1 == 2 && nh == 6) return launch_l<2, 6>;
-  if (n1 == 1 && nh == 5) return launch_l<1, 5>;
-  if (n1 == 1 && nh == 6) return launch_l<1, 6>;
-  if (n1 == 0 && nh == 6) return launch_l<0, 6>;
-  if (n1 == 1 && nh == 3) return launch_l<1, 3>;
+template <class T>
+LaunchL<T> pick_l(int n1, int nh) {
+  if (n1 == 2 && nh == 5) return fit_l<T, 2, 5>();
+  if (n1 == 2 && nh == 3) return fit_l<T, 2, 3>();
+  if (n1 == 2 && nh == 4) return fit_l<T, 2, 4>();
+  if (n1 == 2 && nh == 6) return fit_l<T, 2, 6>();
+  if (n1 == 1 && nh == 5) return fit_l<T, 1, 5>();
+  if (n1 == 1 && nh == 6) return fit_l<T, 1, 6>();
+  if (n1 == 0 && nh == 6) return fit_l<T, 0, 6>();
+  if (n1 == 1 && nh == 3) return fit_l<T, 1, 3>();
   return nullptr;
 }
-LaunchR pick_r(int n1, int nh) {
-  if (n1 == 1 && nh == 6) return launch_r<1, 6>;
-  if (n1 == 1 && nh == 4) return launch_r<1, 4>;
-  if (n1 == 1 && nh == 5) return launch_r<1, 5>;
-  if (n1 == 1 && nh == 3) return launch_r<1, 3>;
-  if (n1 == 1 && nh == 2) return launch_r<1, 2>;
-  if (n1 == 2 && nh == 5) return launch_r<2, 5>;
-  if (n1 == 0 && nh == 6) return launch_r<0, 6>;
-  if (n1 == 0 && nh == 3) return launch_r<0, 3>;
+template <class T>
+LaunchR<T> pick_r(int n1, int nh) {
+  if (n1 == 1 && nh == 6) return fit_r<T, 1, 6>();
+  if (n1 == 1 && nh == 4) return fit_r<T, 1, 4>();
+  if (n1 == 1 && nh == 5) return fit_r<T, 1, 5>();
+  if (n1 == 1 && nh == 3) return fit_r<T, 1, 3>();
+  if (n1 == 1 && nh == 2) return fit_r<T, 1, 2>();
+  if (n1 == 2 && nh == 5) return fit_r<T, 2, 5>();
+  if (n1 == 0 && nh == 6) return fit_r<T, 0, 6>();
+  if (n1 == 0 && nh == 3) return fit_r<T, 0, 3>();
   return nullptr;
 }
 
@@ -678,7 +744,8 @@ void fast_plan_add(CubePlan& p, const rpm_system* s, bool first) {
   int n1l, nhl, n1r, nhr;
   side_pattern(s->cube_l, n1l, nhl);
   side_pattern(s->cube_r, n1r, nhr);
-  bool ok = s->cube && n1l >= 0 && n1r >= 0 && pick_l(n1l, nhl) && pick_r(n1r, nhr) && s->half_r % 8 == 0;
+  bool ok = s->cube && n1l >= 0 && n1r >= 0 && pick_l<float2>(n1l, nhl) && pick_r<float2>(n1r, nhr) &&
+            s->half_r % 8 == 0;
   if (ok) {
     // standard layout: offl[l] = eA * N/2 + l_lo * HR, offr[r] = eB * N/4 + r_lo
     const long long n = s->n, hl = s->half_l, hr = s->half_r;
@@ -700,25 +767,37 @@ void fast_plan_add(CubePlan& p, const rpm_system* s, bool first) {
   }
 }
 
-bool cube_fast_usable(const HpsiArgs<float2>& a, const CubePlan& p, const float2* ya) {
+template <class T>
+bool cube_fast_usable(const HpsiArgs<T>& a, const CubePlan& p, const T* ya) {
   if (!p.fast) return false;
   const long long yld = a.ya_ld ? a.ya_ld : a.ld;
   auto aligned = [](const void* ptr) { return (reinterpret_cast<uintptr_t>(ptr) & 15u) == 0; };
-  if ((a.ld & 1) || (yld & 1) || !aligned(a.in) || !aligned(a.out) || !aligned(ya)) return false;
-  if (a.lz.on == 1 && !a.lz.first && !aligned(a.lz.prev)) return false;
-  return pick_l(p.fl_n1, p.fl_nh) && pick_r(p.fr_n1, p.fr_nh);
+  if (!aligned(a.in) || !aligned(a.out) || !aligned(ya)) return false;
+  if constexpr (FastT<T>::EPU == 2) {
+    if ((a.ld & 1) || (yld & 1)) return false;
+    if (a.lz.on == 1 && !a.lz.first && !aligned(a.lz.prev)) return false;
+  } else {
+    if (a.lz.on) return false;  // the fused recurrence is complex64 only
+  }
+  return pick_l<T>(p.fl_n1, p.fl_nh) && pick_r<T>(p.fr_n1, p.fr_nh);
 }
 
-bool launch_cube_fast(const HpsiArgs<float2>& a, const CubePlan& p, float2* ya, int batch, cudaStream_t st) {
-  if (!cube_fast_usable(a, p, ya)) return false;
-  const LaunchL fl = pick_l(p.fl_n1, p.fl_nh);
-  const LaunchR fr = pick_r(p.fr_n1, p.fr_nh);
-  HpsiArgs<float2> ar = a;
+template <class T>
+bool launch_cube_fast(const HpsiArgs<T>& a, const CubePlan& p, T* ya, int batch, cudaStream_t st) {
+  if (!cube_fast_usable<T>(a, p, ya)) return false;
+  const LaunchL<T> fl = pick_l<T>(p.fl_n1, p.fl_nh);
+  const LaunchR<T> fr = pick_r<T>(p.fr_n1, p.fr_nh);
+  HpsiArgs<T> ar = a;
   ar.dot_part = nullptr;
   fr(ar, ya, p.f_half_l, batch, st);
   fl(a, ya, p.f_half_r, batch, st);
   return true;
 }
+
+template bool cube_fast_usable<float2>(const HpsiArgs<float2>&, const CubePlan&, const float2*);
+template bool cube_fast_usable<double2>(const HpsiArgs<double2>&, const CubePlan&, const double2*);
+template bool launch_cube_fast<float2>(const HpsiArgs<float2>&, const CubePlan&, float2*, int, cudaStream_t);
+template bool launch_cube_fast<double2>(const HpsiArgs<double2>&, const CubePlan&, double2*, int, cudaStream_t);
 
 }  // namespace rpm
 

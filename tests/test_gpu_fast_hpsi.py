@@ -97,3 +97,31 @@ def test_fast_path_not_claimed_for_other_axis_orders(rb):
     assert not h2._system.fast_hpsi
     v = synthetic.random_phase_vectors(full.dimensions, 1, 5)[0]
     assert _rel(_apply64(rb, h2, [v], full.dimension)[0], h2.matvec(v)) < REL64
+
+
+@pytest.mark.parametrize("idx", [0, 2, 3])
+def test_complex128_fast_passes_match_general_cube_kernels(rb, idx):
+    """complex128 H psi on the shape-specialised passes (the default for the standard layout) against the
+    general cube kernels (forced through the tuning hook), batched, with a strided leading dimension."""
+    import torch
+
+    from rpm_b200 import _lib
+
+    name, _, h = _systems(rb)[idx]
+    n = h.dimension
+    ld = n + 64
+    rng = np.random.default_rng(17 + idx)
+    x = torch.zeros((3, ld), dtype=torch.complex128, device="cuda")
+    x[:, :n] = torch.from_numpy(rng.normal(size=(3, n)) + 1j * rng.normal(size=(3, n)))
+    fast, general = torch.zeros_like(x), torch.zeros_like(x)
+    _lib.call("rpm_hpsi", h._system.handle, _lib.PREC_C128, _lib.ptr(x), _lib.ptr(fast), 3, ld, _lib.stream_handle())
+    try:
+        _lib.call("rpm_set_cube_tuning", 2, 2, 0, 0)  # any explicit choice bypasses the specialised passes
+        _lib.call("rpm_hpsi", h._system.handle, _lib.PREC_C128, _lib.ptr(x), _lib.ptr(general), 3, ld,
+                  _lib.stream_handle())
+    finally:
+        _lib.call("rpm_set_cube_tuning", 0, 0, 0, 0)
+    torch.cuda.synchronize()
+    assert h._system.fast_hpsi
+    for b in range(3):
+        assert _rel(fast[b, :n].cpu().numpy(), general[b, :n].cpu().numpy()) < 1e-13, name
