@@ -17,9 +17,10 @@
 //   pass R: yb = sf (1 (x) R) psi            pass L: out = sf (L (x) 1 + P) psi + yb
 // but the thread mapping is chosen so that every coefficient a warp needs at
 // a time is the same for all 32 lanes:
-//   * pass R: a CTA stages 32 rows (eA, l) x all (eB, r) of one vector; lane
-//     = row.  R's coefficients depend on (eB, r) only, which is uniform in a
-//     warp task, so they are shared-memory broadcasts.  Each thread holds a
+//   * pass R: a CTA stages 16 rows (eA, l) x all (eB, r) of one vector; lane
+//     bits 0-3 = row, bit 4 = one of the two outer indices of a warp task.
+//     R's coefficients depend on (eB, r) only, which is uniform in a warp
+//     task, so they are shared-memory broadcasts.  Each thread holds a
 //     register cube (eB x the two fastest spin-1/2 digits) of its row.
 //   * pass L: a CTA stages every l of 16 columns (eB x 8 consecutive r);
 //     lane = column (+ one spin-1/2 digit of l as lane bit 4).  L's
@@ -33,7 +34,8 @@
 // beta_{j-1} v_{j-1} (staged there for the combine) from the partial, so
 // pass L never reads v_{j-1}.  Pass L walks the batch in reverse order so
 // that the partials and inputs written or read last are still in L2 when it
-// starts.
+// starts.  complex128 runs the same passes with one element per 16-byte copy,
+// an odd row stride in 16-byte units, no fused recurrence and one CTA per SM.
 #include <utility>
 #include <vector>
 
