@@ -263,7 +263,9 @@ int rpm_batch_leading_dimension(const rpm_batch* batch, long long* ld);
 /* Propagate `ntraj` trajectories; trajectory b uses system sys_of_host[b] and
  * starts from psi_dev + b*ld (complex128, overwritten with the final state).
  * values_dev / state_errors_dev (ntraj x ntimes, FP64, device) receive the
- * singlet population and the accumulated state-error estimate at each time. */
+ * singlet population and the accumulated state-error estimate at each time;
+ * stats_host (ntraj entries, host) receives each trajectory's statistics and
+ * status. */
 int rpm_batch_propagate(rpm_batch* batch, int ntraj, const int* sys_of_host, void* psi_dev,
                         const double* times_host, int ntimes, double* values_dev,
                         double* state_errors_dev, rpm_batch_stats* stats_host, void* stream);
