@@ -79,3 +79,4 @@ def test_complex128_tiles_fit_shared_memory_for_the_full_system():
     hl, hr = half(2, 5), half(1, 6)
     assert 2 * hl * 16 * 16 < limit
     assert 16 * (2 * hr + 1) * 16 < limit
+
