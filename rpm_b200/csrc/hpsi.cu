@@ -23,7 +23,11 @@
 //
 // * Generic per-term mode product for systems without a radical split.
 #include <algorithm>
+#include <atomic>
+#include <mutex>
 #include <type_traits>
+#include <utility>
+#include <vector>
 
 #include "common.cuh"
 #include "hpsi.cuh"
@@ -638,38 +642,58 @@ __global__ void __launch_bounds__(512) split_pass_b(SplitView<T> s, const T* __r
 // Launch planning
 // ---------------------------------------------------------------------------
 int sm_count() {
-  static int count = 0;
-  if (!count) {
-    int dev = 0;
-    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
-    check_cuda(cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
-  }
+  static std::mutex m;
+  static std::vector<std::pair<int, int>> cache;  // (device, SM count)
+  int dev = 0;
+  check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+  std::lock_guard<std::mutex> lock(m);
+  for (const auto& c : cache)
+    if (c.first == dev) return c.second;
+  int count = 0;
+  check_cuda(cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+  cache.emplace_back(dev, count);
   return count;
 }
 
 static constexpr size_t kMaxSmem = 200 * 1024;
 
-// Explicit cube-kernel variant (0 = heuristic), set by rpm_set_cube_tuning.
+// Explicit cube-kernel variant (0 = heuristic), set by rpm_set_cube_tuning;
+// one atomic word (a byte per field) so that a launch reads a consistent set.
 struct CubeTuning {
   int ni_l, ni_r, tr, tl;
 };
-static CubeTuning g_cube_tuning{0, 0, 0, 0};
+static std::atomic<unsigned> g_cube_tuning{0u};
+
+static CubeTuning cube_tuning() {
+  const unsigned v = g_cube_tuning.load(std::memory_order_relaxed);
+  return CubeTuning{(int)(v & 0xffu), (int)((v >> 8) & 0xffu), (int)((v >> 16) & 0xffu), (int)(v >> 24)};
+}
 
 // Raise a kernel's dynamic shared-memory limit only when needed, so that
 // launches recorded into a CUDA graph issue no attribute calls once warmed up.
+// The attribute belongs to the device's context: the cache is per device.
 template <class K>
 static void ensure_smem(K kern, size_t bytes, const char* what) {
-  static std::vector<std::pair<const void*, size_t>> done;
+  struct Done {
+    const void* kernel;
+    int device;
+    size_t bytes;
+  };
+  static std::mutex m;
+  static std::vector<Done> done;
+  int dev = 0;
+  check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
   const void* key = reinterpret_cast<const void*>(kern);
+  std::lock_guard<std::mutex> lock(m);
   for (auto& d : done)
-    if (d.first == key) {
-      if (d.second >= bytes) return;
+    if (d.kernel == key && d.device == dev) {
+      if (d.bytes >= bytes) return;
       check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes), what);
-      d.second = bytes;
+      d.bytes = bytes;
       return;
     }
   check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes), what);
-  done.emplace_back(key, bytes);
+  done.push_back(Done{key, dev, bytes});
 }
 
 template <class T, int NI, int TR>
@@ -701,8 +725,8 @@ static bool try_cube_r(const HpsiArgs<T>& a, const CubePlan& p, const T* ya, int
 // Column-tile width for pass L: as wide as shared memory allows, but narrow
 // enough that small batches still produce about two CTAs per SM.
 template <class T, int NI>
-static void cube_l_dispatch(const HpsiArgs<T>& a, const CubePlan& p, T* ya, int batch, cudaStream_t st) {
-  switch (g_cube_tuning.tr) {  // explicit choice (autotuner); falls back to the heuristic if it cannot run
+static void cube_l_dispatch(const HpsiArgs<T>& a, const CubePlan& p, T* ya, int batch, cudaStream_t st, int tuned_tr) {
+  switch (tuned_tr) {  // explicit choice (autotuner); falls back to the heuristic if it cannot run
     case 8: if (try_cube_l<T, NI, 8>(a, p, ya, batch, st)) return; break;
     case 4: if (try_cube_l<T, NI, 4>(a, p, ya, batch, st)) return; break;
     case 2: if (try_cube_l<T, NI, 2>(a, p, ya, batch, st)) return; break;
@@ -719,8 +743,9 @@ static void cube_l_dispatch(const HpsiArgs<T>& a, const CubePlan& p, T* ya, int 
 }
 
 template <class T, int NI>
-static void cube_r_dispatch(const HpsiArgs<T>& a, const CubePlan& p, const T* ya, int batch, cudaStream_t st) {
-  switch (g_cube_tuning.tl) {
+static void cube_r_dispatch(const HpsiArgs<T>& a, const CubePlan& p, const T* ya, int batch, cudaStream_t st,
+                            int tuned_tl) {
+  switch (tuned_tl) {
     case 16: if (try_cube_r<T, NI, 16>(a, p, ya, batch, st)) return; break;
     case 8: if (try_cube_r<T, NI, 8>(a, p, ya, batch, st)) return; break;
     case 4: if (try_cube_r<T, NI, 4>(a, p, ya, batch, st)) return; break;
@@ -740,23 +765,24 @@ static void cube_r_dispatch(const HpsiArgs<T>& a, const CubePlan& p, const T* ya
 
 template <class T>
 void launch_cube(const HpsiArgs<T>& a, const CubePlan& p, T* ya, int batch, cudaStream_t st) {
-  const bool tuned = g_cube_tuning.ni_l || g_cube_tuning.ni_r || g_cube_tuning.tr || g_cube_tuning.tl;
+  const CubeTuning tu = cube_tuning();
+  const bool tuned = tu.ni_l || tu.ni_r || tu.tr || tu.tl;
   if (!tuned && launch_cube_fast<T>(a, p, ya, batch, st)) return;
-  const int ni_l = g_cube_tuning.ni_l > 0 ? std::min(g_cube_tuning.ni_l, p.ni_l) : p.ni_l;
-  const int ni_r = g_cube_tuning.ni_r > 0 ? std::min(g_cube_tuning.ni_r, p.ni_r) : p.ni_r;
+  const int ni_l = tu.ni_l > 0 ? std::min(tu.ni_l, p.ni_l) : p.ni_l;
+  const int ni_r = tu.ni_r > 0 ? std::min(tu.ni_r, p.ni_r) : p.ni_r;
   if (ni_l >= 2) {
     HpsiArgs<T> al = a;
     al.dot_part = nullptr;
-    cube_l_dispatch<T, 2>(al, p, ya, batch, st);
+    cube_l_dispatch<T, 2>(al, p, ya, batch, st, tu.tr);
   } else {
     HpsiArgs<T> al = a;
     al.dot_part = nullptr;
-    cube_l_dispatch<T, 1>(al, p, ya, batch, st);
+    cube_l_dispatch<T, 1>(al, p, ya, batch, st, tu.tr);
   }
   if (ni_r >= 2) {
-    cube_r_dispatch<T, 2>(a, p, ya, batch, st);
+    cube_r_dispatch<T, 2>(a, p, ya, batch, st, tu.tl);
   } else {
-    cube_r_dispatch<T, 1>(a, p, ya, batch, st);
+    cube_r_dispatch<T, 1>(a, p, ya, batch, st, tu.tl);
   }
 }
 
@@ -907,7 +933,7 @@ extern "C" int rpm_set_cube_tuning(int ni_l, int ni_r, int tr, int tl) {
     };
     if (!ok(ni_l, {0, 1, 2}) || !ok(ni_r, {0, 1, 2}) || !ok(tr, {0, 1, 2, 4, 8}) || !ok(tl, {0, 1, 2, 4, 8, 16}))
       rpm::fail(RPM_E_INVALID, "cube tuning: ni in {0,1,2}, tr in {0,1,2,4,8}, tl in {0,1,2,4,8,16}");
-    rpm::g_cube_tuning = rpm::CubeTuning{ni_l, ni_r, tr, tl};
+    rpm::g_cube_tuning.store((unsigned)ni_l | ((unsigned)ni_r << 8) | ((unsigned)tr << 16) | ((unsigned)tl << 24));
   });
 }
 

@@ -36,6 +36,7 @@
 // that the partials and inputs written or read last are still in L2 when it
 // starts.  complex128 runs the same passes with one element per 16-byte copy,
 // an odd row stride in 16-byte units, no fused recurrence and one CTA per SM.
+#include <mutex>
 #include <utility>
 #include <vector>
 
@@ -656,10 +657,12 @@ __global__ void __launch_bounds__(PassL<T, N1, NH>::WARPS * 32, FastT<T>::MINB)
 // launches recorded into a CUDA graph issue no attribute calls.
 template <class K>
 void set_smem(K kern, int bytes) {
+  static std::mutex m;
   static std::vector<std::pair<const void*, int>> done;  // (kernel, device)
   int dev = 0;
   check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
   const void* key = reinterpret_cast<const void*>(kern);
+  std::lock_guard<std::mutex> lock(m);
   for (const auto& d : done)
     if (d.first == key && d.second == dev) return;
   check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes), "fast H psi smem attr");
