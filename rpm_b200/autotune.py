@@ -37,6 +37,9 @@ from .batched import BatchedPropagator
 from .engine import _torch
 
 KRYLOV_RANGE = (16, 24, 32, 40)      # the batched configuration's Krylov cap range
+# Every cap the batched path accepts (its limit is 64): larger caps take
+# longer Krylov steps for the same per-step controller work.
+KRYLOV_EXTENDED = (16, 24, 32, 40, 48, 56, 64)
 TILE_RANGE = (8, 16, 32, 48, 64)     # trajectories per batch
 
 

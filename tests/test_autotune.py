@@ -18,6 +18,14 @@ def test_budget_meets_the_population_bound():
         budget_for_yield_tolerance(0.0)
 
 
+def test_krylov_ranges_stay_within_the_batched_limit():
+    from rpm_b200.autotune import KRYLOV_EXTENDED, KRYLOV_RANGE
+
+    assert KRYLOV_RANGE == (16, 24, 32, 40)  # the batched benchmark configuration's cap range
+    assert set(KRYLOV_RANGE) <= set(KRYLOV_EXTENDED)
+    assert min(KRYLOV_EXTENDED) >= 2 and max(KRYLOV_EXTENDED) == 64
+
+
 @pytest.mark.gpu
 def test_tune_picks_a_candidate_and_caches(tmp_path):
     import rpm_b200 as rb
