@@ -801,6 +801,55 @@ def mixed_two_electron_log_negativity(rho) -> float:
 
 
 # ---------------------------------------------------------------------------
+# Closed-form yields from a dense spectrum
+# ---------------------------------------------------------------------------
+def _singlet_rows(vectors: np.ndarray, nuclear_dimension: int) -> np.ndarray:
+    """Singlet amplitudes (psi[1, k] - psi[2, k]) / sqrt(2) of each column of
+    ``vectors`` (electron-major layout, electrons on axes 0 and 1)."""
+    m = nuclear_dimension
+    return (vectors[m:2 * m] - vectors[2 * m:3 * m]) / math.sqrt(2.0)
+
+
+def truncated_singlet_yield_dense(h_dense, dimensions: Sequence[int], psi0, lifetime_us: float,
+                                  final_time_us: float) -> float:
+    """(1/tau) int_0^T exp(-t/tau) P_S(t) dt in closed form for a Hermitian dense H.
+
+    With psi(t) = sum_n c_n exp(-i E_n t)|n> and s_kn the singlet amplitudes of
+    eigenvector n, P_S(t) = sum_nm conj(c_n) c_m (s^H s)_nm exp(i (E_n - E_m) t),
+    and each term integrates to r (1 - exp(-(r - i w) T)) / (r - i w) with
+    r = 1/tau, w = E_n - E_m.  CORE:455-473 (dense_truncated_singlet_yield)
+    is the four-level case with the singlet as initial state.
+    """
+    dims = tuple(int(v) for v in dimensions)
+    m = math.prod(dims) // 4
+    energies, vectors = np.linalg.eigh(np.asarray(h_dense, dtype=complex))
+    coeff = vectors.conj().T @ np.asarray(psi0, dtype=complex)
+    rows = _singlet_rows(vectors, m)
+    gram = rows.conj().T @ rows
+    weights = np.conj(coeff)[:, None] * coeff[None, :] * gram
+    rate = 1.0 / float(lifetime_us)
+    decay = rate - 1j * (energies[:, None] - energies[None, :])
+    integral = rate * (1.0 - np.exp(-decay * float(final_time_us))) / decay
+    return float(np.sum(weights * integral).real)
+
+
+def ensemble_singlet_yield_lorentzian(h_dense, dimensions: Sequence[int], lifetime_us: float) -> float:
+    """Infinite-horizon singlet yield of the singlet (x) maximally mixed nuclear
+    ensemble from the spectrum: W_nm = |<n|P_S|m>|^2 / M (M nuclear states) and
+    sum_nm W_nm / (1 + tau^2 (E_n - E_m)^2) --
+    rpm_three_nitrogen_quadrupole.py:100-113 (QuadrupoleModel.spectrum, .yields).
+    """
+    dims = tuple(int(v) for v in dimensions)
+    m = math.prod(dims) // 4
+    energies, vectors = np.linalg.eigh(np.asarray(h_dense, dtype=complex))
+    rows = _singlet_rows(vectors, m)
+    weights = np.abs(rows.conj().T @ rows) ** 2 / m
+    gaps2 = (energies[:, None] - energies[None, :]) ** 2
+    tau = float(lifetime_us)
+    return float(np.sum(weights / (1.0 + tau * tau * gaps2)))
+
+
+# ---------------------------------------------------------------------------
 # Unequal Haberkorn rates (no reference implementation: dense restatement)
 # ---------------------------------------------------------------------------
 def haberkorn_dense(h_dense, dimensions: Sequence[int], psi0, times_us, singlet_rate: float, triplet_rate: float):
