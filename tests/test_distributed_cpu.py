@@ -3,7 +3,6 @@
 import os
 import socket
 
-import numpy as np
 import pytest
 
 from rpm_b200.distributed import gather_yields, max_over_ranks, shard_bounds, trajectory_costs

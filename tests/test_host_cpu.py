@@ -1,10 +1,8 @@
 """Host-side checks that need no GPU: the C ABI library, its host-built
 radical-split tables, and the Python model/assembly code."""
 
-import ctypes
 import math
 import re
-from pathlib import Path
 
 import numpy as np
 import pytest

@@ -10,7 +10,6 @@ file is named so that pytest collects it last.
 import ctypes
 import math
 
-import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
