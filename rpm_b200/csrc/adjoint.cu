@@ -600,6 +600,8 @@ extern "C" int rpm_adjoint_create(int ntraj, long long n, long long ld, int degr
     if (degree < 1 || degree > kAdjMaxDegree) fail(RPM_E_INVALID, "Taylor degree must be in [1, 24]");
     if (nodes < 1 || nodes > kAdjMaxNodes) fail(RPM_E_INVALID, "quadrature nodes must be in [1, 4]");
     if (precision != RPM_PREC_C64 && precision != RPM_PREC_C128) fail(RPM_E_INVALID, "precision must be 64 or 128");
+    int device = 0;
+    check_cuda(cudaGetDevice(&device), "cudaGetDevice");
     auto* a = new rpm_adjoint();
     a->B = ntraj;
     a->n = n;
@@ -608,7 +610,7 @@ extern "C" int rpm_adjoint_create(int ntraj, long long n, long long ld, int degr
     a->nodes = nodes;
     a->precision = precision;
     a->elem = precision == RPM_PREC_C64 ? sizeof(float2) : sizeof(double2);
-    check_cuda(cudaGetDevice(&a->device), "cudaGetDevice");
+    a->device = device;
     auto alloc = [&](void** p, size_t bytes, const char* what) {
       if (cudaMalloc(p, bytes) != cudaSuccess) {
         cudaGetLastError();

@@ -1478,6 +1478,24 @@ static void run_batch(rpm_batch* Bh, int ntraj, const int* sys_of, void* psi, co
   }
 }
 
+// Frees everything a batch owns (also a partly created one) and the batch.
+static void release_batch(rpm_batch* batch) {
+  free_graph(batch);
+  if (batch->work) cudaStreamSynchronize(batch->work);
+  if (batch->side) cudaStreamSynchronize(batch->side);
+  if (batch->buf) cudaFree(batch->buf);
+  if (batch->views_dev) cudaFree(batch->views_dev);
+  if (batch->ev_fork) cudaEventDestroy(batch->ev_fork);
+  if (batch->ev_join) cudaEventDestroy(batch->ev_join);
+  if (batch->side) cudaStreamDestroy(batch->side);
+  if (batch->ev_in) cudaEventDestroy(batch->ev_in);
+  if (batch->ev_out) cudaEventDestroy(batch->ev_out);
+  if (batch->probe0) cudaEventDestroy(batch->probe0);
+  if (batch->probe1) cudaEventDestroy(batch->probe1);
+  if (batch->work) cudaStreamDestroy(batch->work);
+  delete batch;
+}
+
 }  // namespace rpm
 
 using namespace rpm;
@@ -1492,7 +1510,7 @@ int rpm_batch_create(rpm_system* const* systems, int nsys, const rpm_batch_confi
     if (cfg->embedded_offset < 1 || cfg->embedded_offset >= cfg->krylov_dim)
       fail(RPM_E_INVALID, "embedded offset must be in [1, krylov_dim)");
     if (!(cfg->state_error_budget > 0.0) || !(cfg->maximum_step_us > 0.0)) fail(RPM_E_INVALID, "bad step controls");
-    auto B = std::make_unique<rpm_batch>();
+    std::unique_ptr<rpm_batch, void (*)(rpm_batch*)> B(new rpm_batch(), release_batch);
     B->cfg = *cfg;
     std::vector<CubeView<float2>> views;
     for (int k = 0; k < nsys; ++k) {
@@ -1566,20 +1584,7 @@ int rpm_batch_set_budget(rpm_batch* batch, double state_error_budget) {
 int rpm_batch_destroy(rpm_batch* batch) {
   return guarded([&] {
     if (!batch) return;
-    free_graph(batch);
-    if (batch->work) cudaStreamSynchronize(batch->work);
-    if (batch->side) cudaStreamSynchronize(batch->side);
-    if (batch->buf) cudaFree(batch->buf);
-    if (batch->views_dev) cudaFree(batch->views_dev);
-    if (batch->ev_fork) cudaEventDestroy(batch->ev_fork);
-    if (batch->ev_join) cudaEventDestroy(batch->ev_join);
-    if (batch->side) cudaStreamDestroy(batch->side);
-    if (batch->ev_in) cudaEventDestroy(batch->ev_in);
-    if (batch->ev_out) cudaEventDestroy(batch->ev_out);
-    if (batch->probe0) cudaEventDestroy(batch->probe0);
-    if (batch->probe1) cudaEventDestroy(batch->probe1);
-    if (batch->work) cudaStreamDestroy(batch->work);
-    delete batch;
+    release_batch(batch);
   });
 }
 
