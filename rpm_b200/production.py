@@ -136,38 +136,80 @@ def selected_radicals(nuclear_count: int) -> tuple[str, ...]:
     return ("FAD",) * per + ("TrpH",) * per
 
 
+@dataclass(frozen=True)
+class _BathSite:
+    """One nucleus of the bath: its tensor axis, the electron of its radical
+    (0 = FAD / electron A, 1 = TrpH / electron B) and its "radical:name" key."""
+
+    axis: int
+    electron: int | None
+    key: str
+    nucleus: Nucleus
+
+
+_RADICAL_ELECTRON = {"FAD": 0, "TrpH": 1}
+
+
+def _bath_sites(nuclei: Sequence[Nucleus], radicals: Sequence[str]) -> list[_BathSite]:
+    """Validated site table of a bath prefix.  Error texts and their order are
+    the ones callers of core.py:172-229 match on: a length mismatch first,
+    then duplicate keys, then a radical other than FAD / TrpH."""
+    if len(nuclei) != len(radicals):
+        raise ValueError("nuclei and radicals must have the same length.")
+    sites = [_BathSite(axis, _RADICAL_ELECTRON.get(radical), f"{radical}:{nucleus.name}", nucleus)
+             for axis, (nucleus, radical) in enumerate(zip(nuclei, radicals), start=2)]
+    keys = [site.key for site in sites]
+    if len(set(keys)) != len(keys):
+        raise ValueError("Selected nuclei contain duplicate radical/name keys.")
+    if any(site.electron is None for site in sites):
+        raise ValueError("Every selected nucleus must belong to FAD or TrpH.")
+    return sites
+
+
+def production_terms(theta_deg: float, field_mT: float, *, coupling: ElectronCoupling = PRODUCTION_COUPLING,
+                     quadrupole_scale: float = 1.0, nuclei: Sequence[Nucleus] = ALL_NUCLEI,
+                     radicals: Sequence[str] = NUCLEAR_RADICALS,
+                     hyperfine_overrides_mT: dict[str, np.ndarray] | None = None):
+    """(dimensions, terms, left_axes, right_axes) of the production
+    Hamiltonian; host-only, see :func:`build_hamiltonian`.
+
+    Same operator and term labels as core.py:172-229 (labels and error texts
+    are matched by callers); assembled from the validated site table: the two
+    electron Zeeman terms, then per site its hyperfine term and, where the
+    site has a quadrupole tensor and the scale is nonzero, its quadrupole
+    term, then the electron-pair coupling.  The radical split groups each
+    electron with the sites of its radical.
+    """
+    sites = _bath_sites(nuclei, radicals)
+    overrides = hyperfine_overrides_mT or {}
+    to_rad = TWOPI * GAMMA_E_MHZ_PER_MT  # mT -> rad/us
+    zeeman = _zeeman(theta_deg, float(field_mT) * 1000.0)
+    terms = [LocalTerm((e,), zeeman, f"electron {name} Zeeman") for e, name in ((0, "A"), (1, "B"))]
+    for site in sites:
+        hf_tensor = np.asarray(overrides.get(site.key, site.nucleus.tensor_mT), dtype=float)
+        terms.append(LocalTerm((site.electron, site.axis),
+                               to_rad * two_spin_coupling_operator(0.5, site.nucleus.spin, hf_tensor),
+                               f"{site.key} hyperfine"))
+        q_tensor = QUADRUPOLE_TENSORS_MT.get(site.key)
+        if q_tensor is not None and quadrupole_scale != 0.0:
+            terms.append(LocalTerm((site.axis,), quadrupole_operator(site.nucleus.spin, to_rad * quadrupole_scale * q_tensor),
+                                   f"{site.key} quadrupole"))
+    pair = efimova_hore_electron_coupling_operator(coupling.exchange_J_MHz, coupling.d_paper_MHz,
+                                                   np.asarray(coupling.dipolar_axis, dtype=float))
+    terms.append(LocalTerm((0, 1), TWOPI * pair, "Efimova-Hore exchange + full nonsecular dipolar"))
+    split = {e: (e,) + tuple(site.axis for site in sites if site.electron == e) for e in (0, 1)}
+    return dimensions_for(nuclei), terms, split[0], split[1]
+
+
 def build_hamiltonian(theta_deg: float, field_mT: float, *, coupling: ElectronCoupling = PRODUCTION_COUPLING,
                       quadrupole_scale: float = 1.0, nuclei: Sequence[Nucleus] = ALL_NUCLEI,
                       radicals: Sequence[str] = NUCLEAR_RADICALS,
                       hyperfine_overrides_mT: dict[str, np.ndarray] | None = None) -> CompiledFullPairHamiltonian:
-    """Production non-factorised Hamiltonian for any paired bath prefix (core.py:172-229)."""
-    if len(nuclei) != len(radicals):
-        raise ValueError("nuclei and radicals must have the same length.")
-    dims = dimensions_for(nuclei)
-    zeeman = _zeeman(theta_deg, float(field_mT) * 1000.0)
-    terms = [LocalTerm((0,), zeeman, "electron A Zeeman"), LocalTerm((1,), zeeman, "electron B Zeeman")]
-    overrides = hyperfine_overrides_mT or {}
-    seen: dict[str, int] = {}
-    for k, (nucleus, radical) in enumerate(zip(nuclei, radicals)):
-        e = 0 if radical == "FAD" else 1
-        key = f"{radical}:{nucleus.name}"
-        tensor = np.asarray(overrides.get(key, nucleus.tensor_mT), dtype=float)
-        terms.append(LocalTerm((e, k + 2), TWOPI * GAMMA_E_MHZ_PER_MT * two_spin_coupling_operator(0.5, nucleus.spin, tensor),
-                               f"{key} hyperfine"))
-        q = QUADRUPOLE_TENSORS_MT.get(key)
-        if q is not None and quadrupole_scale != 0.0:
-            terms.append(LocalTerm((k + 2,), quadrupole_operator(
-                nucleus.spin, TWOPI * GAMMA_E_MHZ_PER_MT * quadrupole_scale * q), f"{key} quadrupole"))
-        seen[key] = seen.get(key, 0) + 1
-    if any(v != 1 for v in seen.values()):
-        raise ValueError("Selected nuclei contain duplicate radical/name keys.")
-    terms.append(LocalTerm((0, 1), TWOPI * efimova_hore_electron_coupling_operator(
-        coupling.exchange_J_MHz, coupling.d_paper_MHz, np.asarray(coupling.dipolar_axis, dtype=float)),
-        "Efimova-Hore exchange + full nonsecular dipolar"))
-    left = (0,) + tuple(k + 2 for k, r in enumerate(radicals) if r == "FAD")
-    right = (1,) + tuple(k + 2 for k, r in enumerate(radicals) if r == "TrpH")
-    if len(left) + len(right) != len(dims):
-        raise ValueError("Every selected nucleus must belong to FAD or TrpH.")
+    """Production non-factorised Hamiltonian of any paired bath prefix on the
+    device (core.py:172-229; term list from :func:`production_terms`)."""
+    dims, terms, left, right = production_terms(theta_deg, field_mT, coupling=coupling,
+                                                quadrupole_scale=quadrupole_scale, nuclei=nuclei, radicals=radicals,
+                                                hyperfine_overrides_mT=hyperfine_overrides_mT)
     return CompiledFullPairHamiltonian(dims, terms, left_axes=left, right_axes=right)
 
 

@@ -2,7 +2,7 @@
 
 Run once with the reference next to the checkout:
 
-    python tests/golden/make_entanglement_golden.py /root/reference
+    python tests/golden/make_entanglement_golden.py <RPM checkout>
 
 It runs the reference's own ``poster_reproduction.core`` functions (through
 ``make_golden.load_reference``) on seeded random states of a 4-nucleus paired
@@ -66,4 +66,6 @@ def main(root: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    if len(sys.argv) != 2:
+        raise SystemExit(f"usage: python {Path(__file__).name} <path of the RPM checkout>")
+    main(Path(sys.argv[1]))

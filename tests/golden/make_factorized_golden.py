@@ -2,7 +2,7 @@
 
 Run once with the reference next to the checkout:
 
-    python tests/golden/make_factorized_golden.py /root/reference
+    python tests/golden/make_factorized_golden.py <RPM checkout>
 
 Runs the reference's own ``rpm_quantum_needle_reproduction`` functions: the
 toy-pair self-test (exact line sum and FFT convolution, run_self_test) and
@@ -52,4 +52,6 @@ def main(root: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    if len(sys.argv) != 2:
+        raise SystemExit(f"usage: python {Path(__file__).name} <path of the RPM checkout>")
+    main(Path(sys.argv[1]))

@@ -2,7 +2,7 @@
 
 Run once in a checkout that has the reference next to it:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <RPM checkout>
 
 It imports ``rpm_statevector_engine`` / ``rpm_quantum_needle_model`` /
 ``poster_reproduction.core`` / ``rpm_quantum_needle_jd_sweeps`` from the
@@ -251,4 +251,6 @@ def main(root: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    if len(sys.argv) != 2:
+        raise SystemExit(f"usage: python {Path(__file__).name} <path of the RPM checkout>")
+    main(Path(sys.argv[1]))

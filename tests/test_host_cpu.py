@@ -145,3 +145,38 @@ def test_batched_shape_order_groups_trajectories_by_shape():
     assert list(order) == [1, 3, 4, 0, 2]  # stable; shapes in the order of the Hamiltonian list
     grouped = np.array([1, 0, 1, 2, 0])[order]
     assert list(grouped) == [0, 2, 0, 1, 1]
+
+
+@pytest.mark.parametrize("count", [4, 8, 14])
+@pytest.mark.parametrize("coupling_ratio,qscale", [(None, 0.0), (-3.0, 1.0)])
+def test_production_terms_match_the_oracle_builder(count, coupling_ratio, qscale):
+    """The production term list (core.py:172-229) agrees with the oracle's
+    restatement term by term: axes, labels, operators and radical split."""
+    from rpm_b200 import production as p
+
+    nuclei = p.selected_nuclei(count) if count < 14 else p.ALL_NUCLEI
+    radicals = p.selected_radicals(count) if count < 14 else p.NUCLEAR_RADICALS
+    coupling = p.UNCOUPLED if coupling_ratio is None else p.ElectronCoupling.ratio(coupling_ratio)
+    dims, terms, left, right = p.production_terms(37.0, 0.05, coupling=coupling, quadrupole_scale=qscale,
+                                                  nuclei=nuclei, radicals=radicals)
+    ref = oracle.build_hamiltonian(37.0, 0.05, nuclei=nuclei, radicals=radicals, quadrupole_scale=qscale,
+                                   exchange_J_uT=coupling.exchange_J_uT, d_paper_uT=coupling.d_paper_uT,
+                                   dipolar_axis=coupling.dipolar_axis)
+    assert tuple(dims) == tuple(ref.dimensions)
+    assert (tuple(left), tuple(right)) == (tuple(ref.left_axes), tuple(ref.right_axes))
+    assert [t.label for t in terms] == [t.label for t in ref.terms]
+    for t, r in zip(terms, ref.terms):
+        assert tuple(t.axes) == tuple(r.axes)
+        np.testing.assert_allclose(t.operator, r.operator, rtol=0, atol=1e-12)
+
+
+def test_production_terms_error_texts():
+    from rpm_b200 import production as p
+
+    n0, n1 = p.ALL_NUCLEI[0], p.ALL_NUCLEI[1]
+    with pytest.raises(ValueError, match="same length"):
+        p.production_terms(0.0, 0.05, nuclei=(n0,), radicals=("FAD", "TrpH"))
+    with pytest.raises(ValueError, match="duplicate radical/name keys"):
+        p.production_terms(0.0, 0.05, nuclei=(n0, n0), radicals=("FAD", "FAD"))
+    with pytest.raises(ValueError, match="belong to FAD or TrpH"):
+        p.production_terms(0.0, 0.05, nuclei=(n0, n1), radicals=("FAD", "Flavin"))
