@@ -139,13 +139,17 @@ int rpm_bin_transition_lines(const double* lam_dev, const void* sp_dev, const vo
 /* rpm_hpsi without any device allocation.  It has no counterpart in the
  * reference.  It serves callers that may not call cudaMalloc while they run
  * (run loops of frameworks that own all device memory through a pool or
- * arena, fixed-budget embedded runtimes, code running while its owner
- * captures the stream into a CUDA graph).  Its only scratch, batch x ld
- * elements of the partial result between the two radical passes, lives in a 4 MiB array compiled into the
- * library, which every GPU that loads the library keeps until process exit;
- * larger batch x ld x element-size requests fail with RPM_E_UNSUPPORTED.
+ * arena, where a cudaMalloc would synchronise the device and escape their
+ * accounting; fixed-budget embedded runtimes).  It picks the same kernels as
+ * rpm_hpsi for the same arguments.  Its only scratch, batch x ld elements of
+ * the partial result between the two radical passes, lives in a 4 MiB array
+ * compiled into the library, which every GPU that loads the library keeps
+ * until process exit; larger batch x ld x element-size requests fail with
+ * RPM_E_UNSUPPORTED (systems without a radical split need no scratch).
  * The first call on each device looks up that array's device address (and
- * sets kernel attributes); make it before any stream capture.  All calls
+ * sets kernel attributes); make it before any stream capture.  The address
+ * is cached for the device's primary context: do not call it again on a
+ * device after cudaDeviceReset.  All calls
  * share the one array: calls that overlap on the GPU (concurrent streams or
  * threads) race and must be serialised by the caller.  Nothing in the array
  * needs to start at zero; each call overwrites what it reads. */

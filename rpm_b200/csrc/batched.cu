@@ -1055,7 +1055,9 @@ __global__ void __launch_bounds__(256) k_b_observe(BatchDev B) {
 struct rpm_batch {
   std::vector<rpm_system*> systems;
   rpm_batch_config cfg{};
-  rpm::CubePlan plan{};
+  // maxima over all systems of the batch, for buffer sizing only (launches
+  // use the plan of their shape group)
+  int max_nl = 0, max_half_r = 0;
   rpm::CubeView<float2>* views_dev = nullptr;
   long long ld = 0;
   // buffers (grown on demand)
@@ -1321,20 +1323,10 @@ static void run_batch(rpm_batch* Bh, int ntraj, const int* sys_of, void* psi, co
   const int nblk = (int)((Bh->ld + kEwChunk - 1) / kEwChunk);
   const int gblk = std::max(1, std::min(32, (int)((Bh->ld / 4 + kGramChunk - 1) / kGramChunk)));
   // shape groups: runs of consecutive trajectories whose systems share a shape
-  auto same_shape = [](const rpm_system* x, const rpm_system* y) {
-    if (x == y) return true;
-    if (x->n != y->n || x->nl != y->nl || x->nr != y->nr || x->cube_l.K != y->cube_l.K || x->cube_r.K != y->cube_r.K)
-      return false;
-    for (int k = 0; k < x->cube_l.K; ++k)
-      if (x->cube_l.dim[k] != y->cube_l.dim[k]) return false;
-    for (int k = 0; k < x->cube_r.K; ++k)
-      if (x->cube_r.dim[k] != y->cube_r.dim[k]) return false;
-    return x->offl == y->offl && x->offr == y->offr;
-  };
   Bh->groups.clear();
   for (int b = 0; b < ntraj;) {
     int e = b + 1;
-    while (e < ntraj && same_shape(Bh->systems[sys_of[e]], Bh->systems[sys_of[b]])) ++e;
+    while (e < ntraj && same_cube_shape(Bh->systems[sys_of[e]], Bh->systems[sys_of[b]])) ++e;
     std::vector<rpm_system*> members;
     for (int k = b; k < e; ++k) {
       rpm_system* sk = Bh->systems[sys_of[k]];
@@ -1344,7 +1336,7 @@ static void run_batch(rpm_batch* Bh, int ntraj, const int* sys_of, void* psi, co
     b = e;
   }
   // partial-sum slots per trajectory: general pass R (grid.x <= nl) or fused pass L (3 per block)
-  const int dot_blocks = std::max({Bh->plan.nl, 3 * (Bh->plan.half_r / 8), 1});
+  const int dot_blocks = std::max({Bh->max_nl, 3 * (Bh->max_half_r / 8), 1});
   Bh->dot_stride = dot_blocks;
   const Layout L = layout(Bh, ntraj, ntimes, nblk, gblk, dot_blocks);
   if (L.total > Bh->buf_bytes) {
@@ -1519,12 +1511,15 @@ int rpm_batch_create(rpm_system* const* systems, int nsys, const rpm_batch_confi
       if (!s->cube) fail(RPM_E_UNSUPPORTED, "the batched path needs the radical-split cube form");
       if (s->ndims < 2 || s->dims[0] != 2 || s->dims[1] != 2)
         fail(RPM_E_INVALID, "The first two axes must be the two electron spins.");
+      if (s->cube64.inner_l < 1 || s->cube64.inner_r < 1)
+        fail(RPM_E_UNSUPPORTED, "cube kernels need a trailing spin-1/2 digit per radical");
       B->systems.push_back(s);
       views.push_back(s->cube32);
       B->ld = std::max(B->ld, s->n);
+      B->max_nl = std::max(B->max_nl, s->nl);
+      B->max_half_r = std::max(B->max_half_r, s->half_r);
     }
     B->ld = (B->ld + 63) & ~63LL;
-    B->plan = cube_plan(B->systems.data(), nsys);
     check_cuda(cudaStreamCreateWithFlags(&B->work, cudaStreamNonBlocking), "create batch stream");
     check_cuda(cudaEventCreateWithFlags(&B->ev_in, cudaEventDisableTiming), "create event");
     check_cuda(cudaEventCreateWithFlags(&B->ev_out, cudaEventDisableTiming), "create event");

@@ -838,12 +838,29 @@ template <class T> const CubeView<T>* cube_dev_of(rpm_system* sys);
 template <> const CubeView<double2>* cube_dev_of<double2>(rpm_system* sys) { return sys->cube64_dev; }
 template <> const CubeView<float2>* cube_dev_of<float2>(rpm_system* sys) { return sys->cube32_dev; }
 
+bool same_cube_shape(const rpm_system* x, const rpm_system* y) {
+  if (x == y) return true;
+  if (x->n != y->n || x->nl != y->nl || x->nr != y->nr || x->cube_l.K != y->cube_l.K || x->cube_r.K != y->cube_r.K)
+    return false;
+  for (int k = 0; k < x->cube_l.K; ++k)
+    if (x->cube_l.dim[k] != y->cube_l.dim[k]) return false;
+  for (int k = 0; k < x->cube_r.K; ++k)
+    if (x->cube_r.dim[k] != y->cube_r.dim[k]) return false;
+  return x->offl == y->offl && x->offr == y->offr;
+}
+
+// One launch plan covers systems of one shape only: every size, table cap
+// and inner-digit count of the plan is then exactly each member's own, so no
+// per-view quantity of a launch can differ from the plan it was sized by.
+// Batches of uneven sizes launch one plan per shape group.
 CubePlan cube_plan(rpm_system* const* systems, int nsys) {
   CubePlan p{};
   p.ni_l = p.ni_r = 2;
   for (int k = 0; k < nsys; ++k) {
     const rpm_system* s = systems[k];
     if (!s->cube) fail(RPM_E_UNSUPPORTED, "system has no cube form");
+    if (k > 0 && !same_cube_shape(systems[0], s))
+      fail(RPM_E_UNSUPPORTED, "a cube launch plan needs systems of one shape (same dimensions, digits and layout)");
     p.nl = std::max(p.nl, s->nl);
     p.nr = std::max(p.nr, s->nr);
     p.half_r = std::max(p.half_r, s->half_r);
@@ -960,9 +977,9 @@ extern "C" int rpm_hpsi(rpm_system* sys, int precision, const void* psi_dev, voi
 //
 // For callers that must not allocate device memory while they run: host
 // frameworks whose run loop forbids cudaMalloc (their memory comes from a
-// pool or arena they own), embedded runtimes with a fixed memory budget
-// decided at start-up, and code that runs while its owner is capturing a
-// stream into a CUDA graph.  rpm_hpsi grows a per-system cudaMalloc'd buffer
+// pool or arena they own, and a cudaMalloc would synchronise the device and
+// take memory outside their accounting), and embedded runtimes with a fixed
+// memory budget decided at start-up.  rpm_hpsi grows a per-system cudaMalloc'd buffer
 // for the only scratch the radical-split action needs, the partial result
 // (batch x ld elements).  This variant uses a fixed array compiled into the
 // library instead, so every GPU that loads the library holds those bytes
@@ -981,7 +998,10 @@ static std::mutex g_noalloc_mutex;
 
 // Device address of g_noalloc_scratch on the current device.  In host code
 // the array's name is only a host-side stand-in, so the address is looked up
-// once per device, with that device current, and cached.
+// once per device, with that device current, and cached for the life of the
+// device's primary context: after cudaDeviceReset the cached address is
+// stale, so a process that resets a device must not call rpm_hpsi_noalloc on
+// it again.
 static void* noalloc_scratch() {
   int dev = 0;
   check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
@@ -1009,7 +1029,9 @@ static void launch_hpsi_noalloc(rpm_system* sys, const T* in, T* out, int batch,
                                 " bytes exceeds its fixed 4 MiB scratch; use rpm_hpsi or a smaller batch");
   }
   T* ya = static_cast<T*>(noalloc_scratch());
-  if (sys->cube && !sys->non_hermitian && sys->cube64.inner_l >= 1 && sys->cube64.inner_r >= 1) {
+  // the kernel choice of launch_hpsi: cube form, else the CSR passes, else
+  // the per-term kernel (which needs no scratch)
+  if (sys->cube && sys->cube64.inner_l >= 1 && sys->cube64.inner_r >= 1) {
     HpsiArgs<T> a{};
     a.in = in;
     a.out = out;
@@ -1024,7 +1046,7 @@ static void launch_hpsi_noalloc(rpm_system* sys, const T* in, T* out, int batch,
   if (a_ok && (try_pass_b<T, 4, 8>(s, in, ya, out, batch, ld, stream) ||
                try_pass_b<T, 2, 4>(s, in, ya, out, batch, ld, stream)))
     return;
-  fail(RPM_E_UNSUPPORTED, "rpm_hpsi_noalloc: radical groups too large for the shared-memory kernels");
+  launch_generic<T>(generic_of<T>(sys), in, out, batch, ld, stream);
 }
 
 }  // namespace rpm

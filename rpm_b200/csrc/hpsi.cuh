@@ -69,6 +69,9 @@ struct CubePlan {
 };
 
 int sm_count();
+// Same dimensions, digit pattern and layout (offset tables) of the two radicals.
+bool same_cube_shape(const rpm_system* x, const rpm_system* y);
+// Launch plan over systems of ONE shape (fails with RPM_E_UNSUPPORTED otherwise).
 CubePlan cube_plan(rpm_system* const* systems, int nsys);
 void fast_plan_add(CubePlan& p, const rpm_system* s, bool first);
 // Launches the specialised passes; false (nothing launched) when the plan or

@@ -2,9 +2,10 @@
 
 rpm_hpsi_noalloc is for callers that may not call cudaMalloc while they run
 (for example a framework whose run loop owns all device memory through its own
-pool, or code running while its owner captures the stream into a CUDA graph).
-It keeps its scratch in a fixed 4 MiB array compiled into the library.  This
-file is named so that pytest collects it last.
+pool, where a cudaMalloc would synchronise the device and escape the pool's
+accounting).  It keeps its scratch in a fixed 4 MiB array compiled into the
+library and picks the same kernels as rpm_hpsi.  This file is named so that
+pytest collects it last.
 """
 
 import ctypes
@@ -70,3 +71,57 @@ def test_noalloc_rejects_batches_beyond_its_scratch():
     status = fn(h._system.handle, 128, _lib.ptr(x), _lib.ptr(out), 2, n, _lib.stream_handle())
     assert status == _lib.RPM_E_UNSUPPORTED
     assert "4 MiB" in lib.rpm_last_error().decode()
+
+
+def _small_variant(kind):
+    """A 96-dimensional system that takes one kernel route of rpm_hpsi:
+    'csr' (a radical term coupling two nuclei: CSR passes), 'unequal'
+    (unequal recombination rates: the non-Hermitian pair operator on the cube
+    passes) or 'generic' (a cross-radical nuclear term: no radical split, the
+    per-term kernel)."""
+    import numpy as np
+
+    import rpm_b200 as rb
+    from rpm_b200 import synthetic
+
+    small = synthetic.small_system()
+    terms = list(small.terms(0.4, 0.9))
+    rng = np.random.default_rng(8)
+    left, right = small.left_axes[1:], small.right_axes[1:]
+    if kind == "unequal":
+        h = rb.CompiledFullPairHamiltonian(small.dimensions, terms, left_axes=small.left_axes,
+                                           right_axes=small.right_axes)
+        h.set_recombination_rates(1.0, 2.0)
+        return h, small.dimensions
+    if kind == "csr":
+        axes = tuple(left[:2]) if len(left) >= 2 else tuple(right[:2])
+    else:
+        axes = (left[0], right[0])
+    d = small.dimensions[axes[0]] * small.dimensions[axes[1]]
+    a = rng.normal(size=(d, d)) + 1j * rng.normal(size=(d, d))
+    terms.append(rb.LocalTerm(axes, 0.3 * (a + a.conj().T)))
+    return rb.MatrixFreeHamiltonian(small.dimensions, terms), small.dimensions
+
+
+@pytest.mark.parametrize("kind", ["csr", "unequal", "generic"])
+@pytest.mark.parametrize("precision", [128, 64])
+def test_noalloc_takes_every_route_of_the_allocating_entry_point(kind, precision):
+    import torch
+
+    from rpm_b200 import _lib, synthetic
+
+    lib, fn = _entry()
+    h, dims = _small_variant(kind)
+    n = h.dimension
+    batch = 3
+    dtype = torch.complex128 if precision == 128 else torch.complex64
+    x = torch.from_numpy(synthetic.random_phase_vectors(dims, batch, 77)).to("cuda", dtype)
+    expected = torch.empty_like(x)
+    h.apply(x, expected, batch=batch, precision=precision)
+    for _ in range(2):
+        out = torch.full_like(x, float("nan"))
+        status = fn(h._system.handle, precision, _lib.ptr(x), _lib.ptr(out), batch, n, _lib.stream_handle())
+        assert status == 0, lib.rpm_last_error().decode()
+        torch.cuda.synchronize()
+        rel = float(torch.linalg.vector_norm(out - expected) / torch.linalg.vector_norm(expected))
+        assert rel < REL_TOL[precision]
