@@ -244,7 +244,25 @@ typedef struct rpm_batch_config {
   double breakdown_relative;   /* beta_j <= rel*(|alpha_j|+beta_{j-1}): stop */
   int use_graph;               /* replay each Krylov step from a CUDA graph   */
   long long max_steps;         /* safety limit on Krylov steps (<=0: 1e7)    */
+  int lanczos_kernel;          /* RPM_LANCZOS_PERSISTENT (0): one persistent
+                                  launch per Krylov step where the shape has
+                                  one; RPM_LANCZOS_PASSES (1): two pass
+                                  launches per Lanczos iteration             */
+  int wavefront;               /* persistent kernel: vectors that advance
+                                  together through the iterations (<=0: 12) */
+  int reorth_policy;           /* RPM_REORTH_NONE (0): three-term recurrence
+                                  only; RPM_REORTH_PERIODIC (1): after every
+                                  `reorth_period` iterations the next Lanczos
+                                  vector is reorthogonalised against the whole
+                                  basis (two classical Gram-Schmidt passes,
+                                  FP64 sums over the complex64 basis)        */
+  int reorth_period;           /* iterations between reorthogonalisations    */
 } rpm_batch_config;
+
+#define RPM_LANCZOS_PERSISTENT 0
+#define RPM_LANCZOS_PASSES 1
+#define RPM_REORTH_NONE 0
+#define RPM_REORTH_PERIODIC 1
 
 typedef struct rpm_batch_stats {
   int accepted_steps;
@@ -274,11 +292,17 @@ int rpm_batch_propagate(rpm_batch* batch, int ntraj, const int* sys_of_host, voi
                         const double* times_host, int ntimes, double* values_dev,
                         double* state_errors_dev, rpm_batch_stats* stats_host, void* stream);
 /* Measurement counters since creation or the last reset: kernels launched,
- * Krylov-step replays, and the mean duration (ms) of one batched H psi (both
- * passes, all trajectories) sampled inside the graph while no trajectory had
- * finished. */
+ * Krylov-step replays, and the mean duration (ms) of one batched Lanczos
+ * iteration (H psi with the fused recurrence, all trajectories) sampled inside
+ * the graph while no trajectory had finished: one pass pair, or the persistent
+ * launches of a step divided by its iterations. */
 int rpm_batch_counters(rpm_batch* batch, int reset, long long* kernel_launches, long long* step_replays,
                        double* hpsi_ms_mean, long long* hpsi_samples);
+/* How the last recorded Krylov step ran its Lanczos iterations (replaces the
+ * per-vector loop of ENG:651-688): 0 one persistent launch per shape group
+ * (per segment between reorthogonalisations), 1 shape-specialised pass pairs
+ * per iteration, 2 general cube kernels (or Arnoldi). */
+int rpm_batch_lanczos_kind(const rpm_batch* batch, int* kind);
 /* Replace the configured state-error budget for later propagate calls (the
  * knob ENG:620-649 exposes as a mutable attribute). */
 int rpm_batch_set_budget(rpm_batch* batch, double state_error_budget);

@@ -55,7 +55,8 @@ class rpm_batch_config(ctypes.Structure):
                 ("state_error_budget", ctypes.c_double), ("initial_step_us", ctypes.c_double),
                 ("maximum_step_us", ctypes.c_double), ("minimum_step_us", ctypes.c_double),
                 ("breakdown_relative", ctypes.c_double), ("use_graph", ctypes.c_int),
-                ("max_steps", ctypes.c_longlong)]
+                ("max_steps", ctypes.c_longlong), ("lanczos_kernel", ctypes.c_int), ("wavefront", ctypes.c_int),
+                ("reorth_policy", ctypes.c_int), ("reorth_period", ctypes.c_int)]
 
 
 class rpm_batch_stats(ctypes.Structure):
@@ -104,6 +105,7 @@ SIGNATURES: dict[str, list] = {
     "rpm_batch_propagate": [_P, _I, _PI, _P, _PD, _I, _P, _P, ctypes.POINTER(rpm_batch_stats), _P],
     "rpm_batch_destroy": [_P],
     "rpm_batch_set_budget": [_P, _D],
+    "rpm_batch_lanczos_kind": [_P, _PI],
     "rpm_batch_counters": [_P, _I, _PLL, _PLL, _PD, _PLL],
     "rpm_adjoint_create": [_I, _LL, _LL, _I, _I, _I, ctypes.POINTER(_P)],
     "rpm_adjoint_destroy": [_P],

@@ -55,12 +55,23 @@ class BatchedPropagator:
     ``hamiltonians`` are rpm_b200 Hamiltonians with a radical split (for
     example from :func:`rpm_b200.build_hamiltonian` or a
     :class:`CompiledFullPairHamiltonian`); they may differ in dimension.
+
+    ``lanczos_kernel``: "persistent" runs all Lanczos iterations of a Krylov
+    step in one launch per shape group where the shape has a persistent
+    kernel (else the per-iteration passes); "passes" launches the two
+    shape-specialised passes per iteration.  ``wavefront``: vectors that move
+    through the iterations together in the persistent kernel (0: 12).
+    ``reorth_period`` > 0 reorthogonalises the next Lanczos vector against the
+    whole basis after every that many iterations (two classical Gram-Schmidt
+    passes in FP64 over the complex64 basis); 0 keeps the plain three-term
+    recurrence.
     """
 
     def __init__(self, hamiltonians: Sequence[MatrixFreeHamiltonian], *, krylov_dimension: int = 32,
                  embedded_offset: int = 4, safety_factor: float = 2.0, state_error_budget: float = 1e-7,
                  initial_step_us: float = 0.05, maximum_step_us: float = 0.25, minimum_step_us: float = 1e-9,
-                 breakdown_relative: float = 1e-5, use_graph: bool = True, max_steps: int = 0) -> None:
+                 breakdown_relative: float = 1e-5, use_graph: bool = True, max_steps: int = 0,
+                 lanczos_kernel: str = "passes", wavefront: int = 0, reorth_period: int = 0) -> None:
         hams = list(hamiltonians)
         if not hams:
             raise ValueError("At least one Hamiltonian is required.")
@@ -79,6 +90,14 @@ class BatchedPropagator:
         cfg.breakdown_relative = float(breakdown_relative)
         cfg.use_graph = 1 if use_graph else 0
         cfg.max_steps = int(max_steps)
+        if lanczos_kernel not in ("persistent", "passes"):
+            raise ValueError("lanczos_kernel must be 'persistent' or 'passes'")
+        cfg.lanczos_kernel = 0 if lanczos_kernel == "persistent" else 1
+        cfg.wavefront = int(wavefront)
+        if int(reorth_period) < 0:
+            raise ValueError("reorth_period must be >= 0")
+        cfg.reorth_policy = 1 if int(reorth_period) > 0 else 0
+        cfg.reorth_period = int(reorth_period)
         self.config = cfg
         handles = (ctypes.c_void_p * len(hams))(*[h._system.handle.value for h in hams])
         handle = ctypes.c_void_p()
@@ -163,6 +182,14 @@ class BatchedPropagator:
         _lib.call("rpm_batch_counters", self._handle, 1 if reset else 0, ctypes.byref(k), ctypes.byref(r),
                   ctypes.byref(ms), ctypes.byref(n))
         return {"kernel_launches": k.value, "step_replays": r.value, "hpsi_ms": ms.value, "hpsi_samples": n.value}
+
+    def lanczos_kind(self) -> str:
+        """How the last propagation ran its Lanczos iterations: "persistent"
+        (one launch per Krylov step and shape group), "passes" (two
+        shape-specialised launches per iteration) or "cube" (general kernels)."""
+        k = ctypes.c_int()
+        _lib.call("rpm_batch_lanczos_kind", self._handle, ctypes.byref(k))
+        return ("persistent", "passes", "cube")[k.value]
 
     def yields_device(self, times_us, values, lifetime_us: float):
         """Simpson yields of each row of ``values`` on the GPU (FP64, compensated)."""

@@ -74,6 +74,15 @@ struct BatchDev {
   double* errs;     // [traj][ntimes]
   int nblk, gblk;
   int* active;      // trajectories not yet done
+  // persistent Lanczos kernel: per-trajectory progress / tile counters and
+  // L-tile partial sums, one dequeue counter per launch, sticky wait status
+  int* prog;
+  unsigned* pcnt;
+  double* ppart;
+  int ppart_stride;
+  unsigned* work;
+  int nwork;
+  int* kstatus;
   // Arnoldi (non-Hermitian systems: unequal recombination rates)
   int arnoldi;
   double grid_h;    // uniform observation spacing
@@ -182,6 +191,14 @@ __global__ void __launch_bounds__(kEwThreads) k_b_init(BatchDev B) {
 __global__ void __launch_bounds__(kEwThreads) k_b_start(BatchDev B) {
   const int b = blockIdx.y;
   TrajState& s = B.st[b];
+  if (blockIdx.x == 0) {  // persistent-kernel counters start from zero every Krylov step
+    if (threadIdx.x == 0) {
+      B.prog[b] = 0;
+      B.pcnt[b] = 0;
+    }
+    if (b == 0)
+      for (int k = threadIdx.x; k < B.nwork; k += blockDim.x) B.work[k] = 0u;
+  }
   if (s.done) return;
   const double inv = 1.0 / s.norm;
   const double2* x = B.psi + (size_t)b * B.ld;
@@ -680,6 +697,114 @@ __global__ void __launch_bounds__(kEwThreads) k_b_arn_axpy(BatchDev B, int j, in
   }
 }
 
+// ---------------------------------------------------------------------------
+// Periodic reorthogonalisation of the Lanczos recurrence (reorth_policy 1)
+// ---------------------------------------------------------------------------
+// After iteration j the next vector is r = w'_(j+1) - alpha_j v_j, with w' held
+// in V_(j+1).  One classical Gram-Schmidt pass against v_0 .. v_j:
+// k_b_reo_dots forms d_i = <v_i, r> (FP64 sums of FP32 products, per-block
+// partials summed in block order by the last block), k_b_reo_axpy stores
+// w' - sum_i d_i v_i (so that r becomes r - sum_i d_i v_i) and, after the
+// second pass, sets beta_j = |r| and the next scale (the reference runs two
+// such passes every iteration, rpm_statevector_engine.py:675-676).
+__global__ void __launch_bounds__(kEwThreads) k_b_reo_dots(BatchDev B, int j) {
+  __shared__ double2 red[kEwThreads / 32][kBMaxK];
+  const int b = blockIdx.y;
+  TrajState& s = B.st[b];
+  if (s.skip) return;
+  const float2* base = B.V + (size_t)b * (B.m + 1) * B.ld;
+  const float2* w = base + (size_t)(j + 1) * B.ld;
+  const float2* vj = base + (size_t)j * B.ld;
+  const float al = (float)s.alpha[j];
+  const long long i0 = (long long)blockIdx.x * kEwChunk + threadIdx.x;
+  float2 rv[kEwPer];
+#pragma unroll
+  for (int k = 0; k < kEwPer; ++k) {
+    const long long e = i0 + (long long)k * kEwThreads;
+    rv[k] = make_float2(0.f, 0.f);
+    if (e < s.n) {
+      const float2 x = w[e], v = vj[e];
+      rv[k] = make_float2(fmaf(-al, v.x, x.x), fmaf(-al, v.y, x.y));
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int i = 0; i <= j; ++i) {
+    const float2* v = base + (size_t)i * B.ld;
+    double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int k = 0; k < kEwPer; ++k) {
+      const long long e = i0 + (long long)k * kEwThreads;
+      if (e < s.n) {
+        const float2 q = v[e];  // conj(q) * r
+        acc.x += (double)q.x * rv[k].x + (double)q.y * rv[k].y;
+        acc.y += (double)q.x * rv[k].y - (double)q.y * rv[k].x;
+      }
+    }
+    acc.x = warp_sum(acc.x);
+    acc.y = warp_sum(acc.y);
+    if (lane == 0) red[warp][i] = acc;
+  }
+  __syncthreads();
+  double2* part = B.adots + ((size_t)b * B.nblk + blockIdx.x) * kBMaxK;
+  for (int i = threadIdx.x; i <= j; i += blockDim.x) {
+    double2 t = make_double2(0.0, 0.0);
+    for (int w2 = 0; w2 < kEwThreads / 32; ++w2) t = cadd(t, red[w2][i]);
+    part[i] = t;
+  }
+  if (traj_last_block(B.count + b)) {
+    for (int i = threadIdx.x; i <= j; i += blockDim.x) {
+      double2 t = make_double2(0.0, 0.0);
+      for (int k = 0; k < (int)gridDim.x; ++k) t = cadd(t, __ldcg(B.adots + ((size_t)b * B.nblk + k) * kBMaxK + i));
+      B.hcur[(size_t)b * kBMaxK + i] = t;
+    }
+    if (threadIdx.x == 0) B.count[b] = 0;
+  }
+}
+
+__global__ void __launch_bounds__(kEwThreads) k_b_reo_axpy(BatchDev B, int j, int last_pass) {
+  __shared__ float2 hc[kBMaxK];
+  __shared__ double red[32];
+  const int b = blockIdx.y;
+  TrajState& s = B.st[b];
+  if (s.skip) return;
+  for (int i = threadIdx.x; i <= j; i += blockDim.x) {
+    const double2 t = B.hcur[(size_t)b * kBMaxK + i];
+    hc[i] = make_float2((float)t.x, (float)t.y);
+  }
+  __syncthreads();
+  float2* base = B.V + (size_t)b * (B.m + 1) * B.ld;
+  float2* w = base + (size_t)(j + 1) * B.ld;
+  const float2* vj = base + (size_t)j * B.ld;
+  const float al = (float)s.alpha[j];
+  double nn = 0.0;
+  const long long end = min(s.n, (long long)(blockIdx.x + 1) * kEwChunk);
+  for (long long e = (long long)blockIdx.x * kEwChunk + threadIdx.x; e < end; e += kEwThreads) {
+    float2 x = w[e];
+    for (int i = 0; i <= j; ++i) x = cfma(make_float2(-hc[i].x, -hc[i].y), base[(size_t)i * B.ld + e], x);
+    w[e] = x;
+    const float2 v = vj[e];
+    const float rx = fmaf(-al, v.x, x.x), ry = fmaf(-al, v.y, x.y);
+    nn = fma((double)rx, (double)rx, fma((double)ry, (double)ry, nn));
+  }
+  if (!last_pass) return;
+  nn = block_sum(nn, red);
+  if (threadIdx.x == 0) B.part[((size_t)b * B.nblk + blockIdx.x) * 2] = nn;
+  if (traj_last_block(B.count + b) && threadIdx.x == 0) {
+    double tot = 0.0;
+    for (int k = 0; k < (int)gridDim.x; ++k) tot += __ldcg(B.part + ((size_t)b * B.nblk + k) * 2);
+    const double beta = sqrt(tot);
+    s.beta[j] = beta;
+    s.scale = beta > 0.0 ? 1.0 / beta : 0.0;
+    const double ref = fabs(s.alpha[j]) + (j > 0 ? s.beta[j - 1] : 0.0);
+    if (!(beta > B.breakdown_rel * ref)) {
+      s.stop = 1;
+      s.skip = 1;
+      s.msize = j + 1;
+    }
+    B.count[b] = 0;
+  }
+}
+
 // Matrix product C = A X for n x n complex matrices in shared memory (row-major).
 __device__ void cmatmul(int n, const double2* A, const double2* X, double2* C) {
   for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
@@ -1084,7 +1209,9 @@ struct rpm_batch {
   long long probe_samples = 0;
   long long kernel_launches = 0, replays = 0;
   int launches_per_step = 0;
-  bool fused = false;  // every group runs the fused passes
+  int probe_iters = 1;      // Lanczos iterations between the probe events
+  bool fused = false;       // every group runs the fused passes
+  bool persistent = false;  // every group runs the persistent Lanczos kernel
   // Consecutive trajectories whose systems share one shape (digit pattern and
   // layout) form a group; each group's H psi is one launch pair with its own
   // plan, on the shape-specialised passes when the shape allows.
@@ -1108,10 +1235,11 @@ static void free_graph(rpm_batch* B) {
 
 struct Layout {
   size_t st, V, coef, perr, part, count, gpart, ya, dotpart, dotcount, times, sysof, nof, active, hess, hcur, adots,
-      expm, total;
+      expm, prog, pcnt, ppart, work, kstatus, total;
 };
 
-static Layout layout(const rpm_batch* B, int ntraj, int ntimes, int nblk, int gblk, int dot_blocks) {
+static Layout layout(const rpm_batch* B, int ntraj, int ntimes, int nblk, int gblk, int dot_blocks, int ppart_stride,
+                     int nwork) {
   Layout L{};
   size_t pos = 0;
   auto take = [&](size_t bytes) {
@@ -1138,6 +1266,11 @@ static Layout layout(const rpm_batch* B, int ntraj, int ntimes, int nblk, int gb
   L.hcur = take(sizeof(double2) * (size_t)ntraj * kBMaxK);
   L.adots = take(sizeof(double2) * (size_t)ntraj * nblk * kBMaxK);
   L.expm = take(sizeof(double2) * (size_t)ntraj * 2 * kBMaxK * kBMaxK);
+  L.prog = take(sizeof(int) * ntraj);
+  L.pcnt = take(sizeof(unsigned) * ntraj);
+  L.ppart = take(sizeof(double) * (size_t)ntraj * ppart_stride);
+  L.work = take(sizeof(unsigned) * (size_t)nwork);
+  L.kstatus = take(sizeof(int));
   L.total = pos;
   return L;
 }
@@ -1238,6 +1371,8 @@ static void record_step(rpm_batch* Bh, const BatchDev& B, const Layout& L, cudaS
       }
     }
     Bh->fused = false;
+    Bh->persistent = false;
+    Bh->probe_iters = 1;
     Bh->launches_per_step = 1 + (per_iter + 4) * m + 4;
     check_cuda(cudaEventRecord(Bh->ev_fork, st), "fork record");
     check_cuda(cudaStreamWaitEvent(Bh->side, Bh->ev_fork, 0), "fork wait");
@@ -1250,7 +1385,80 @@ static void record_step(rpm_batch* Bh, const BatchDev& B, const Layout& L, cudaS
     check_launch("batched Arnoldi step");
     return;
   }
-  for (int j = 0; j < m; ++j) {
+  // Shape groups with a persistent Lanczos kernel run every iteration of the
+  // step in one launch; the others launch their passes per iteration.
+  // Periodic reorthogonalisation after iterations P-1, 2P-1, ... (< m-1)
+  // covers every trajectory at once: with it, either every group runs the
+  // persistent kernel (in segments between the reorthogonalisations) or none.
+  const int reo = Bh->cfg.reorth_policy == RPM_REORTH_PERIODIC && Bh->cfg.reorth_period > 0 ? Bh->cfg.reorth_period : 0;
+  std::vector<char> gpers(Bh->groups.size());
+  int npers = 0;
+  for (size_t g = 0; g < Bh->groups.size(); ++g) {
+    gpers[g] = Bh->cfg.lanczos_kernel == RPM_LANCZOS_PERSISTENT && gfused[g] &&
+               persistent_l_tiles(Bh->groups[g].plan) > 0;
+    npers += gpers[g];
+  }
+  if (reo > 0 && npers != (int)Bh->groups.size()) {
+    std::fill(gpers.begin(), gpers.end(), 0);
+    npers = 0;
+  }
+  const bool all_pers = npers == (int)Bh->groups.size();
+  auto reorth_after = [&](int j) { return reo > 0 && (j + 1) % reo == 0 && j + 1 < m; };
+  auto reorthogonalise = [&](int j) {
+    for (int pass = 1; pass <= 2; ++pass) {
+      k_b_reo_dots<<<ew, kEwThreads, 0, st>>>(B, j);
+      k_b_reo_axpy<<<ew, kEwThreads, 0, st>>>(B, j, pass == 2 ? 1 : 0);
+    }
+    check_launch("batched reorthogonalisation");
+  };
+  const int nseg = reo > 0 ? (m + reo - 1) / reo : 1;  // segments of the persistent launches
+  if (all_pers) check_cuda(cudaEventRecordWithFlags(Bh->probe0, st, probe_flags), "probe record");
+  for (int seg = 0; seg < nseg && npers > 0; ++seg) {
+    const int j0 = reo > 0 ? seg * reo : 0;
+    const int j1 = reo > 0 ? std::min(m, (seg + 1) * reo) : m;
+    for (size_t g = 0; g < Bh->groups.size(); ++g) {
+      if (!gpers[g]) continue;
+      const auto& G = Bh->groups[g];
+      PersistentLanczos P{};
+      P.V = B.V + (size_t)G.b0 * (m + 1) * B.ld;
+      P.ld = B.ld;
+      P.vstride = (long long)(m + 1) * B.ld;
+      P.slot0 = (long long)G.b0 * (m + 1);
+      P.m = m;
+      P.nb = G.nb;
+      P.gv = Bh->cfg.wavefront > 0 ? Bh->cfg.wavefront : 12;
+      P.j0 = j0;
+      P.j1 = j1;
+      P.views = Bh->views_dev;
+      P.sys_of = reinterpret_cast<const int*>(base + L.sysof) + G.b0;
+      P.alpha = &B.st[G.b0].alpha[0];
+      P.beta = &B.st[G.b0].beta[0];
+      P.scale = &B.st[G.b0].scale;
+      P.dstride = kStateDoubles;
+      P.stop = &B.st[G.b0].stop;
+      P.skip = &B.st[G.b0].skip;
+      P.msize = &B.st[G.b0].msize;
+      P.istride = kStateInts;
+      P.breakdown_rel = B.breakdown_rel;
+      P.ya = ya + (size_t)G.b0 * B.ld;
+      P.prog = B.prog + G.b0;
+      P.cnt = B.pcnt + G.b0;
+      P.part = B.ppart + (size_t)G.b0 * B.ppart_stride;
+      P.part_stride = B.ppart_stride;
+      P.work = B.work + g * nseg + seg;
+      P.status = B.kstatus;
+      if (!launch_lanczos_persistent(P, G.plan, B.V, (long long)B.ntraj * (m + 1), st))
+        fail(RPM_E_INVALID, "persistent Lanczos kernel unavailable");
+    }
+    if (all_pers && reorth_after(j1 - 1)) reorthogonalise(j1 - 1);
+  }
+  if (all_pers) {
+    check_cuda(cudaEventRecordWithFlags(Bh->probe1, st, probe_flags), "probe record");
+    Bh->probe_iters = m;
+  } else {
+    Bh->probe_iters = 1;
+  }
+  for (int j = 0; j < m && !all_pers; ++j) {
     a.in = B.V + (size_t)j * B.ld;
     a.out = B.V + (size_t)(j + 1) * B.ld;
     // While capturing, external records become event-record nodes of the graph.
@@ -1274,6 +1482,7 @@ static void record_step(rpm_batch* Bh, const BatchDev& B, const Layout& L, cudaS
     z.istride = kStateInts;
     z.breakdown_rel = B.breakdown_rel;
     for (size_t g = 0; g < Bh->groups.size(); ++g) {
+      if (gpers[g]) continue;
       const auto& G = Bh->groups[g];
       HpsiArgs<float2> ak = group_args(a, G.b0, D);
       float2* yk = ya + (size_t)G.b0 * B.ld;
@@ -1287,11 +1496,17 @@ static void record_step(rpm_batch* Bh, const BatchDev& B, const Layout& L, cudaS
         k_b_update<<<dim3(B.nblk, G.nb), kEwThreads, 0, st>>>(B, j, G.b0);
       }
     }
+    if (reorth_after(j)) reorthogonalise(j);
     if (j == probe_j) check_cuda(cudaEventRecordWithFlags(Bh->probe1, st, probe_flags), "probe record");
   }
   const bool fused = all_fused;
   Bh->fused = fused;
-  Bh->launches_per_step = 1 + per_iter * m + 4;
+  Bh->persistent = all_pers;
+  int per_iter_rest = 0;
+  for (size_t g = 0; g < Bh->groups.size(); ++g)
+    if (!gpers[g]) per_iter_rest += gfused[g] ? 2 : 3;
+  const int nreo = reo > 0 ? (m - 1) / reo : 0;  // iterations j = P-1, 2P-1, ... <= m-2
+  Bh->launches_per_step = 1 + npers * nseg + per_iter_rest * m + 4 * nreo + 4;
   const size_t ctl_smem = sizeof(double) * 2 * kRecDoubles;
   check_cuda(cudaEventRecord(Bh->ev_fork, st), "fork record");
   check_cuda(cudaStreamWaitEvent(Bh->side, Bh->ev_fork, 0), "fork wait");
@@ -1338,7 +1553,13 @@ static void run_batch(rpm_batch* Bh, int ntraj, const int* sys_of, void* psi, co
   // partial-sum slots per trajectory: general pass R (grid.x <= nl) or fused pass L (3 per block)
   const int dot_blocks = std::max({Bh->max_nl, 3 * (Bh->max_half_r / 8), 1});
   Bh->dot_stride = dot_blocks;
-  const Layout L = layout(Bh, ntraj, ntimes, nblk, gblk, dot_blocks);
+  int lt_max = 1;
+  for (const auto& G : Bh->groups) lt_max = std::max(lt_max, persistent_l_tiles(G.plan));
+  const int ppart_stride = 3 * lt_max;
+  const int reo_period = cfg.reorth_policy == RPM_REORTH_PERIODIC && cfg.reorth_period > 0 ? cfg.reorth_period : 0;
+  const int nseg_max = reo_period > 0 ? (cfg.krylov_dim + reo_period - 1) / reo_period : 1;
+  const int nwork = (int)Bh->groups.size() * std::max(1, nseg_max);
+  const Layout L = layout(Bh, ntraj, ntimes, nblk, gblk, dot_blocks, ppart_stride, nwork);
   if (L.total > Bh->buf_bytes) {
     free_graph(Bh);
     if (Bh->buf) check_cuda(cudaFree(Bh->buf), "cudaFree(batch)");
@@ -1349,6 +1570,7 @@ static void run_batch(rpm_batch* Bh, int ntraj, const int* sys_of, void* psi, co
   char* base = static_cast<char*>(Bh->buf);
   check_cuda(cudaMemsetAsync(base + L.count, 0, sizeof(unsigned) * ntraj, st), "memset counters");
   check_cuda(cudaMemsetAsync(base + L.dotcount, 0, sizeof(unsigned) * ntraj, st), "memset counters");
+  check_cuda(cudaMemsetAsync(base + L.kstatus, 0, sizeof(int), st), "memset status");
   check_cuda(cudaMemcpyAsync(base + L.times, times_host, sizeof(double) * ntimes, cudaMemcpyHostToDevice, st), "times");
   check_cuda(cudaMemcpyAsync(base + L.sysof, sys_of, sizeof(int) * ntraj, cudaMemcpyHostToDevice, st), "sys_of");
   check_cuda(cudaMemcpyAsync(base + L.nof, n_of.data(), sizeof(long long) * ntraj, cudaMemcpyHostToDevice, st), "n_of");
@@ -1384,6 +1606,13 @@ static void run_batch(rpm_batch* Bh, int ntraj, const int* sys_of, void* psi, co
   B.hcur = reinterpret_cast<double2*>(base + L.hcur);
   B.adots = reinterpret_cast<double2*>(base + L.adots);
   B.expm = reinterpret_cast<double2*>(base + L.expm);
+  B.prog = reinterpret_cast<int*>(base + L.prog);
+  B.pcnt = reinterpret_cast<unsigned*>(base + L.pcnt);
+  B.ppart = reinterpret_cast<double*>(base + L.ppart);
+  B.ppart_stride = ppart_stride;
+  B.work = reinterpret_cast<unsigned*>(base + L.work);
+  B.nwork = nwork;
+  B.kstatus = reinterpret_cast<int*>(base + L.kstatus);
   B.arnoldi = 0;
   for (rpm_system* sy : Bh->systems) B.arnoldi |= sy->non_hermitian ? 1 : 0;
   B.grid_h = 0.0;
@@ -1437,8 +1666,11 @@ static void run_batch(rpm_batch* Bh, int ntraj, const int* sys_of, void* psi, co
       ++replays;
       Bh->kernel_launches += Bh->launches_per_step;
     }
+    int kstatus = 0;
     check_cuda(cudaMemcpyAsync(&active, base + L.active, sizeof(int), cudaMemcpyDeviceToHost, st), "poll");
+    check_cuda(cudaMemcpyAsync(&kstatus, base + L.kstatus, sizeof(int), cudaMemcpyDeviceToHost, st), "poll");
     check_cuda(cudaStreamSynchronize(st), "poll sync");
+    if (kstatus) fail(RPM_E_TIMEOUT, "persistent Lanczos kernel: a device wait gave up (time limit)");
     if (active == ntraj) {
       float ms = 0.f;
       if (cudaEventElapsedTime(&ms, Bh->probe0, Bh->probe1) == cudaSuccess) {
@@ -1559,12 +1791,20 @@ int rpm_batch_counters(rpm_batch* batch, int reset, long long* kernel_launches, 
     if (!batch) fail(RPM_E_INVALID, "batch is NULL");
     if (kernel_launches) *kernel_launches = batch->kernel_launches;
     if (step_replays) *step_replays = batch->replays;
-    if (hpsi_ms_mean) *hpsi_ms_mean = batch->probe_samples ? batch->probe_ms_sum / batch->probe_samples : 0.0;
+    if (hpsi_ms_mean)
+      *hpsi_ms_mean = batch->probe_samples ? batch->probe_ms_sum / batch->probe_samples / batch->probe_iters : 0.0;
     if (hpsi_samples) *hpsi_samples = batch->probe_samples;
     if (reset) {
       batch->kernel_launches = batch->replays = batch->probe_samples = 0;
       batch->probe_ms_sum = 0.0;
     }
+  });
+}
+
+int rpm_batch_lanczos_kind(const rpm_batch* batch, int* kind) {
+  return guarded([&] {
+    if (!batch || !kind) fail(RPM_E_INVALID, "bad arguments");
+    *kind = batch->persistent ? 0 : batch->fused ? 1 : 2;
   });
 }
 

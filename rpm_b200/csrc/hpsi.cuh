@@ -68,6 +68,51 @@ struct CubePlan {
   int fl_n1, fl_nh, fr_n1, fr_nh, f_half_l, f_half_r;
 };
 
+// One persistent launch runs the Lanczos iterations j0 <= j < j1 of a Krylov
+// step for the trajectories of one shape group on the shape-specialised
+// complex64 passes (lanczos_persistent.cu).  Vector b (0-based in the group)
+// keeps its basis at V + b * vstride + j * ld, its pass-R partial at
+// ya + b * ld and its scalars in the batch's per-trajectory records
+// (ptr + b * dstride [+ j] for doubles, ptr + b * istride for ints).
+// prog/cnt/part/work/status are device scratch: prog, cnt and *work start at
+// zero for every Krylov step (k_b_start), *status at zero for every
+// propagation (nonzero: a wait gave up).
+struct PersistentLanczos {
+  float2* V;
+  long long ld, vstride;
+  long long slot0;  // tensor-map slot of (vector 0, j = 0): vector b, slot j is slot0 + b (m + 1) + j
+  int m, nb, gv;    // Krylov dimension, vectors, vectors per wavefront group
+  int j0, j1;       // iterations j0 <= j < j1 of this launch (a segment of 0 .. m-1)
+  const CubeView<float2>* views;
+  const int* sys_of;
+  double* alpha;  // alpha_j of vector b at alpha[b * dstride + j]
+  double* beta;
+  double* scale;  // 1 / beta_{j-1} of vector b at scale[b * dstride]
+  int dstride;
+  int* stop;
+  int* skip;
+  int* msize;
+  int istride;
+  double breakdown_rel;
+  float2* ya;
+  int* prog;       // per vector: phases completed (R of iteration j -> 2j + 1, L -> 2j + 2)
+  unsigned* cnt;   // per vector: tiles completed in the current phase
+  double* part;    // per vector: [L tile][3] partial sums at part + b * part_stride
+  int part_stride;
+  unsigned* work;  // dequeue counter of this launch
+  int* status;     // sticky wait-timeout flag
+};
+
+// Launches the persistent Lanczos kernel for the plan's shape; false (nothing
+// launched) when no persistent instance exists for it.  `V_base` and
+// `nslots` describe the whole basis buffer ([nslots][ld] complex64) that the
+// tensor map covers.
+bool launch_lanczos_persistent(const PersistentLanczos& p, const CubePlan& plan, const float2* V_base,
+                               long long nslots, cudaStream_t stream);
+// L tiles per vector and iteration of the persistent kernel for a shape (8
+// columns per electron-B half each), 0 when the shape has no instance.
+int persistent_l_tiles(const CubePlan& plan);
+
 int sm_count();
 // Same dimensions, digit pattern and layout (offset tables) of the two radicals.
 bool same_cube_shape(const rpm_system* x, const rpm_system* y);

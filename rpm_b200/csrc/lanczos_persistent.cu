@@ -1,0 +1,563 @@
+// Persistent Lanczos kernel: the iterations of one Krylov step for every
+// trajectory of a shape group in ONE launch (the batched path's dominant
+// work; the reference's per-vector loop is rpm_statevector_engine.py:651-688,
+// its H psi :221-253).
+//
+// Work items are tiles of the two shape-specialised passes (hpsi_fast.cuh):
+//   R(j, b, t): rows 16t .. 16t+15 of vector b, iteration j -- forms
+//               v_j = (w'_j - alpha_{j-1} v_{j-1}) / beta_{j-1} (j > 0),
+//               writes it back and writes the right-radical partial;
+//   L(j, b, t): columns 8t .. 8t+7 of both electron-B halves -- applies the
+//               left radical and the pair operator, adds the partial, writes
+//               w'_{j+1} and reduces <v_j, w'>, |w'|^2, |v_j|^2; the last L
+//               tile of (j, b) sets alpha_j, beta_j and the breakdown flags.
+// One CTA per SM dequeues items from a global counter in a fixed order:
+// vectors in wavefront groups of gv, each group through all iterations of
+// the launch (all m, or a segment between two reorthogonalisations), every
+// iteration as R tiles of the group's vectors, then their L tiles.  A phase
+// of vector b starts only after the phase before it has completed on every
+// CTA (per-vector progress counters); in this order an item only ever depends
+// on items dequeued before it, so every wait ends, and the vectors of one
+// group stay in L2 between the phases.  Every wait has a time limit, after
+// which the kernel sets a sticky status word and drains.
+//
+// Inside a CTA one producer warp dequeues, waits for the item's dependencies
+// and stages it with the Tensor Memory Accelerator into one of two shared-
+// memory stages (mbarrier transaction counts): pass-R rows by bulk copies into
+// padded rows, pass-L columns by 5-D tensor copies, the coefficient table by a
+// bulk copy.  Eight consumer warps compute the other stage meanwhile.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "hpsi.cuh"
+#include "hpsi_fast.cuh"
+
+namespace rpm {
+namespace {
+
+using namespace fastpass;
+
+constexpr int kConsumerWarps = 8;
+constexpr int kConsumers = kConsumerWarps * 32;
+constexpr int kThreads = kConsumers + 32;        // + one producer warp
+constexpr long long kWaitCycles = 4000000000LL;  // about 2 s at 1.965 GHz
+
+constexpr int align128c(int b) { return (b + 127) & ~127; }
+constexpr int cmax(int a, int b) { return a > b ? a : b; }
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// PTX helpers: mbarrier, bulk / tensor copies, acquire / release
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Wait for phase `parity` of `bar` to complete; false after the time limit
+// or when another thread already raised the status word.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, int* status) {
+  const long long t0 = clock64();
+  for (int spin = 0;; ++spin) {
+    if (mbar_test(bar, parity)) return true;
+    if ((spin & 63) == 63) {
+      if (*reinterpret_cast<volatile int*>(status)) return false;
+      if (clock64() - t0 > kWaitCycles) {
+        atomicExch(status, 1);
+        return false;
+      }
+    }
+  }
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_5d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3, int c4,
+                                       unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, "
+      "%6}], [%7];\n" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
+      : "memory");
+}
+// Order this thread's generic-proxy global accesses with async-proxy (TMA)
+// accesses.
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async;\n" ::: "memory"); }
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+// Barrier over the consumer warps only (the producer warp never joins it);
+// returns the AND of `ok` over them.
+__device__ __forceinline__ bool consumers_and(bool ok) {
+  unsigned r;
+  asm volatile(
+      "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.and.pred q, 1, %2, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+      : "=r"(r)
+      : "r"((unsigned)ok), "r"(kConsumers)
+      : "memory");
+  return r != 0;
+}
+__device__ __forceinline__ void consumers_sync() { asm volatile("bar.sync 1, %0;\n" ::"r"(kConsumers) : "memory"); }
+
+// Wait until *p >= need (acquire); false after the time limit or a raised status.
+__device__ bool wait_progress(const int* p, int need, int* status) {
+  const long long t0 = clock64();
+  while (true) {
+    if (ld_acquire(p) >= need) return true;
+    if (*reinterpret_cast<volatile int*>(status)) return false;
+    if (clock64() - t0 > kWaitCycles) {
+      atomicExch(status, 1);
+      return false;
+    }
+    __nanosleep(128);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Shape constants
+// ---------------------------------------------------------------------------
+// Left radical (N1L spin-1, NHL spin-1/2 digits) -> pass L; right radical -> pass R.
+template <int N1L, int NHL, int N1R, int NHR>
+struct PShape {
+  using PR = PassR<float2, N1R, NHR>;
+  using PL = PassL<float2, N1L, NHL>;
+  using SR = typename PR::S;
+  using SL = typename PL::S;
+  static constexpr int HL = PL::HL, HR = PR::HR;
+  static constexpr int TR = PR::TR;                  // rows per R tile
+  static constexpr int RT = (2 * HL + TR - 1) / TR;  // R tiles per vector
+  static constexpr int LT = HR / 8;                  // L tiles per vector
+  static constexpr int PT = RT + LT;
+  // l extent of one tensor-copy box (<= 256 rows, dividing HL)
+  static constexpr int LSPLIT = (HL + 255) / 256;
+  static constexpr int BL = HL / LSPLIT;
+  static_assert(HL % LSPLIT == 0, "l extent must split into equal tensor boxes");
+  static_assert(HR % 8 == 0, "pass L tiles need 8 | HR");
+  static constexpr int TAB_BYTES = align128c(cmax(SR::NTAB, SL::NTAB) * 8);
+  static constexpr int OREC_BYTES = align128c(cmax(PR::NO, PL::NO) * (int)sizeof(ORec<float2>));
+  static constexpr int R_TILE_BYTES = TR * PR::RS * 8;  // one padded R tile
+  static constexpr int L_TILE_BYTES = 2 * HL * 16 * 8;
+  static constexpr int TILE_BYTES = align128c(cmax(2 * R_TILE_BYTES, L_TILE_BYTES));
+  static constexpr int STAGE = TAB_BYTES + OREC_BYTES + TILE_BYTES;
+  static constexpr int SMEM = 2 * STAGE + 1024;  // + alignment slack
+};
+
+struct Item {
+  int kind;  // 0: R, 1: L, -1: end
+  int j, b, tile, skip;
+};
+
+// Item index -> (phase, iteration within the launch, vector, tile) in the
+// wavefront order over `mseg` iterations.
+template <class PS>
+__device__ __forceinline__ Item decode(long long idx, int mseg, int nb, int gv) {
+  Item it{};
+  const long long full_groups = nb / gv;
+  const long long per_group = (long long)mseg * gv * PS::PT;
+  long long vg, r;
+  int g;
+  if (idx < full_groups * per_group) {
+    vg = idx / per_group;
+    r = idx - vg * per_group;
+    g = gv;
+  } else {
+    vg = full_groups;
+    r = idx - full_groups * per_group;
+    g = nb - (int)full_groups * gv;
+  }
+  it.j = (int)(r / ((long long)g * PS::PT));
+  int q = (int)(r - (long long)it.j * g * PS::PT);
+  if (q < g * PS::RT) {
+    it.kind = 0;
+    it.b = (int)vg * gv + q / PS::RT;
+    it.tile = q % PS::RT;
+  } else {
+    q -= g * PS::RT;
+    it.kind = 1;
+    it.b = (int)vg * gv + q / PS::LT;
+    it.tile = q % PS::LT;
+  }
+  return it;
+}
+
+template <int N1L, int NHL, int N1R, int NHR>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_lanczos_persistent(const __grid_constant__ CUtensorMap vmap, PersistentLanczos p) {
+  using PS = PShape<N1L, NHL, N1R, NHR>;
+  using PR = typename PS::PR;
+  using PL = typename PS::PL;
+  constexpr int HL = PS::HL, HR = PS::HR, TR = PS::TR, RS = PR::RS;
+  constexpr long long QUARTER = (long long)HL * HR;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  __shared__ __align__(8) unsigned long long full_bar[2], empty_bar[2];
+  __shared__ Item meta[2];
+  __shared__ double red[kConsumerWarps][3];
+  auto stage_tab = [&](int s) { return reinterpret_cast<float2*>(base + s * PS::STAGE); };
+  auto stage_orec = [&](int s) { return reinterpret_cast<ORec<float2>*>(base + s * PS::STAGE + PS::TAB_BYTES); };
+  auto stage_tile = [&](int s) {
+    return reinterpret_cast<float2*>(base + s * PS::STAGE + PS::TAB_BYTES + PS::OREC_BYTES);
+  };
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < 2; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  const int mseg = p.j1 - p.j0;
+  const long long total = (long long)mseg * p.nb * PS::PT;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (warp == kConsumerWarps) {
+    // ----------------------------- producer -----------------------------
+    // per stage: the last use armed (copies, skip or end) and whether it got copies
+    long long armed_use[2] = {-1, -1};
+    bool armed_copies[2] = {false, false};
+    for (long long it = 0;; ++it) {
+      const int s = (int)(it & 1);
+      const long long use = it >> 1;
+      bool ok = true;
+      if (use >= 1 && lane == 0) ok = mbar_wait(&empty_bar[s], (unsigned)((use - 1) & 1), p.status);
+      long long idx = 0;
+      if (lane == 0 && ok) idx = atomicAdd(p.work, 1u);
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      idx = __shfl_sync(0xffffffffu, idx, 0);
+      Item m{};
+      m.kind = -1;
+      if (ok && idx < total) {
+        m = decode<PS>(idx, mseg, p.nb, p.gv);
+        m.j += p.j0;
+        if (lane == 0) {
+          const int need = m.kind == 0 ? 2 * m.j : 2 * m.j + 1;
+          if (need > 0) ok = wait_progress(p.prog + m.b, need, p.status);
+          m.skip = ok ? *reinterpret_cast<volatile int*>(p.skip + (long long)m.b * p.istride) : 1;
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        m.skip = __shfl_sync(0xffffffffu, m.skip, 0);
+        if (!ok) m.kind = -1;
+      }
+      armed_use[s] = use;
+      armed_copies[s] = !(m.kind < 0 || m.skip);
+      if (m.kind < 0 || m.skip) {
+        if (lane == 0) {
+          meta[s] = m;
+          mbar_arrive(&full_bar[s]);
+        }
+        __syncwarp();
+        if (m.kind < 0) break;
+        continue;
+      }
+      // stage the item's data
+      fence_proxy_async();
+      const CubeView<float2>* view = p.views + (p.sys_of ? p.sys_of[m.b] : 0);
+      const float2* vj = p.V + (long long)m.b * p.vstride + (long long)m.j * p.ld;
+      float2* tile = stage_tile(s);
+      if (m.kind == 0) {
+        const int row0 = m.tile * TR;
+        const int rows = min(TR, 2 * HL - row0);
+        const bool prev = m.j > 0;
+        const unsigned bytes = (unsigned)(rows * 2 * HR * 8 * (prev ? 2 : 1) + PS::SR::NTAB * 8);
+        if (lane == 0) {
+          meta[s] = m;
+          mbar_arrive_expect_tx(&full_bar[s], bytes);
+        }
+        __syncwarp();
+        if (lane == 0) bulk_g2s(stage_tab(s), view->tabR, PS::SR::NTAB * 8, &full_bar[s]);
+        const int rr = lane & 15, which = lane >> 4;
+        if (rr < rows && (which == 0 || prev)) {
+          const float2* src = which == 0 ? vj : vj - p.ld;
+          float2* dst = tile + which * TR * RS + rr * RS;
+          const int rho = row0 + rr;
+          const int ea = rho >= HL ? 1 : 0;
+          const long long g = 2 * ea * QUARTER + (long long)(rho - ea * HL) * HR;
+          bulk_g2s(dst, src + g, HR * 8, &full_bar[s]);
+          bulk_g2s(dst + HR, src + g + QUARTER, HR * 8, &full_bar[s]);
+        }
+      } else {
+        const unsigned bytes = (unsigned)(PS::L_TILE_BYTES + PS::SL::NTAB * 8);
+        if (lane == 0) {
+          meta[s] = m;
+          mbar_arrive_expect_tx(&full_bar[s], bytes);
+        }
+        __syncwarp();
+        if (lane == 0) bulk_g2s(stage_tab(s), view->tabL, PS::SL::NTAB * 8, &full_bar[s]);
+        if (lane < 2 * PS::LSPLIT) {
+          const int ea = lane / PS::LSPLIT, part = lane % PS::LSPLIT;
+          const long long slot = p.slot0 + (long long)m.b * (p.m + 1) + m.j;
+          tma_5d(tile + (ea * HL + part * PS::BL) * 16, &vmap, m.tile * 8, 0, part * PS::BL, ea, (int)slot,
+                 &full_bar[s]);
+        }
+      }
+      __syncwarp();
+    }
+    // drain: copies this warp issued complete before the CTA may exit (a
+    // stage armed again later was consumed, so its copies completed)
+    if (lane == 0) {
+      for (int s = 0; s < 2; ++s)
+        if (armed_copies[s]) mbar_wait(&full_bar[s], (unsigned)(armed_use[s] & 1), p.status);
+    }
+    return;
+  }
+
+  // ----------------------------- consumers -----------------------------
+  const int tid = threadIdx.x;  // 0 .. kConsumers - 1
+  for (long long it = 0;; ++it) {
+    const int s = (int)(it & 1);
+    const unsigned parity = (unsigned)((it >> 1) & 1);
+    const bool ok = consumers_and(mbar_wait(&full_bar[s], parity, p.status));
+    if (!ok) break;
+    const Item m = meta[s];
+    if (m.kind < 0) break;
+    float2* tab = stage_tab(s);
+    ORec<float2>* orec = stage_orec(s);
+    float2* tile = stage_tile(s);
+    const int b = m.b;
+    const CubeView<float2>* view = p.views + (p.sys_of ? p.sys_of[b] : 0);
+    float2* vj = p.V + (long long)b * p.vstride + (long long)m.j * p.ld;
+    float2* yb = p.ya + (long long)b * p.ld;
+    double dot = 0.0, nw = 0.0, nv = 0.0;
+    if (!m.skip) {
+      if (m.kind == 0) {
+        const int row0 = m.tile * TR;
+        const int rows = min(TR, 2 * HL - row0);
+        float2* ptile = tile + TR * RS;
+        const bool prev = m.j > 0;
+        float bprev = 0.0f;
+        if (prev) {
+          // v_j = (w'_j - alpha_{j-1} v_{j-1}) / beta_{j-1}: into the tile and the basis
+          const float al = (float)p.alpha[(long long)b * p.dstride + m.j - 1];
+          const float sc = (float)p.scale[(long long)b * p.dstride];
+          bprev = (float)p.beta[(long long)b * p.dstride + m.j - 1];
+          constexpr int CH = HR / 2;  // 16-byte units per half row
+          for (int u = tid; u < rows * 2 * CH; u += kConsumers) {
+            const int rr = u / (2 * CH), rem = u - rr * (2 * CH);
+            const int e = rem / CH, c = rem - e * CH;
+            const int rho = row0 + rr;
+            const int ea = rho >= HL ? 1 : 0;
+            const int slot = rr * RS + e * HR + 2 * c;
+            const long long g = (2 * ea + e) * QUARTER + (long long)(rho - ea * HL) * HR + 2 * c;
+            const float4 w = *reinterpret_cast<const float4*>(tile + slot);
+            const float4 q = *reinterpret_cast<const float4*>(ptile + slot);
+            float4 v;
+            v.x = sc * fmaf(-al, q.x, w.x);
+            v.y = sc * fmaf(-al, q.y, w.y);
+            v.z = sc * fmaf(-al, q.z, w.z);
+            v.w = sc * fmaf(-al, q.w, w.w);
+            *reinterpret_cast<float4*>(tile + slot) = v;
+            *reinterpret_cast<float4*>(vj + g) = v;
+          }
+        }
+        build_orec<float2, typename PS::SR, PS::SR::K - 2, 4>(tab, orec, PR::NO, tid, kConsumers);
+        consumers_sync();
+        r_tile_math<float2, N1R, NHR>(tab, orec, tile, ptile, rows, row0, HL, QUARTER, yb, 1.0f, bprev, prev, warp,
+                                      kConsumerWarps);
+      } else {
+        build_orec<float2, typename PS::SL, PS::SL::K - 3, 8>(tab, orec, PL::NO, tid, kConsumers);
+        consumers_sync();
+        l_tile_math<float2, N1L, NHL>(tab, orec, tile, view, m.tile * 8, QUARTER, yb, vj + p.ld, 1.0f,
+                                      m.j < p.m - 1, warp, kConsumerWarps, dot, nw, nv);
+        dot = warp_sum_d(dot);
+        nw = warp_sum_d(nw);
+        nv = warp_sum_d(nv);
+        if (lane == 0) {
+          red[warp][0] = dot;
+          red[warp][1] = nw;
+          red[warp][2] = nv;
+        }
+      }
+      // this thread's global writes before the tile is counted, for generic
+      // and tensor-copy readers on other SMs
+      __threadfence();
+      fence_proxy_async();
+    }
+    consumers_sync();
+    if (tid == 0) {
+      const int ntiles = m.kind == 0 ? PS::RT : PS::LT;
+      if (m.kind == 1 && !m.skip) {
+        double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+        for (int w = 0; w < kConsumerWarps; ++w) {
+          t0 += red[w][0];
+          t1 += red[w][1];
+          t2 += red[w][2];
+        }
+        double* part = p.part + (long long)b * p.part_stride + m.tile * 3;
+        part[0] = t0;
+        part[1] = t1;
+        part[2] = t2;
+        __threadfence();
+      }
+      const unsigned done = atomicAdd(p.cnt + b, 1u);
+      if (done == (unsigned)ntiles - 1) {
+        __threadfence();
+        p.cnt[b] = 0;
+        if (m.kind == 1 && !m.skip) {
+          // alpha_j, beta_j and the breakdown test from the tiles' sums, in tile order
+          double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+          const double* part = p.part + (long long)b * p.part_stride;
+          for (int k = 0; k < PS::LT; ++k) {
+            t0 += __ldcg(part + 3 * k);
+            t1 += __ldcg(part + 3 * k + 1);
+            t2 += __ldcg(part + 3 * k + 2);
+          }
+          const double alpha = t2 > 0.0 ? t0 / t2 : 0.0;
+          p.alpha[(long long)b * p.dstride + m.j] = alpha;
+          if (m.j < p.m - 1) {
+            const double beta = sqrt(fmax(t1 - t0 * alpha, 0.0));  // |w' - alpha v_j|
+            p.beta[(long long)b * p.dstride + m.j] = beta;
+            p.scale[(long long)b * p.dstride] = beta > 0.0 ? 1.0 / beta : 0.0;
+            const double ref = fabs(alpha) + (m.j == 0 ? 0.0 : p.beta[(long long)b * p.dstride + m.j - 1]);
+            if (!(beta > p.breakdown_rel * ref)) {
+              p.stop[(long long)b * p.istride] = 1;
+              p.skip[(long long)b * p.istride] = 1;
+              p.msize[(long long)b * p.istride] = m.j + 1;
+            }
+          }
+          __threadfence();
+        }
+        st_release(p.prog + b, m.kind == 0 ? 2 * m.j + 1 : 2 * m.j + 2);
+      }
+      mbar_arrive(&empty_bar[s]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static std::once_flag once;
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    const cudaError_t err = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q);
+    if (err == cudaSuccess && q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    else
+      cudaGetLastError();
+  });
+  if (!fn) fail(RPM_E_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  return fn;
+}
+
+// 5-D map of the basis buffer: (r, eB, l, eA, slot) with strides (element,
+// N/4, HR, N/2, ld) elements and a box of 8 r x 2 eB x BL l, so that one box
+// lands as [l][eB][8 r] rows of 16 elements.
+template <class PS>
+CUtensorMap basis_map(const float2* V, long long nslots, long long ld) {
+  CUtensorMap map;
+  const cuuint64_t q = (cuuint64_t)PS::HL * PS::HR;
+  cuuint64_t dims[5] = {(cuuint64_t)PS::HR, 2, (cuuint64_t)PS::HL, 2, (cuuint64_t)nslots};
+  cuuint64_t strides[4] = {q * 8, (cuuint64_t)PS::HR * 8, 2 * q * 8, (cuuint64_t)ld * 8};
+  cuuint32_t box[5] = {8, 2, (cuuint32_t)PS::BL, 1, 1};
+  cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+  if (nslots < 1 || nslots > 0x7fffffffLL) fail(RPM_E_UNSUPPORTED, "basis too large for the tensor map");
+  const CUresult r = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 5, const_cast<float2*>(V), dims, strides, box,
+                                 estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    fail(RPM_E_CUDA, "cuTensorMapEncodeTiled failed for the basis map (" + std::to_string((int)r) + ")");
+  return map;
+}
+
+template <int N1L, int NHL, int N1R, int NHR>
+void launch_instance(const PersistentLanczos& p, const float2* V_base, long long nslots, cudaStream_t st) {
+  using PS = PShape<N1L, NHL, N1R, NHR>;
+  static_assert(PS::SMEM <= 227 * 1024, "persistent Lanczos stages exceed shared memory");
+  auto kern = k_lanczos_persistent<N1L, NHL, N1R, NHR>;
+  {
+    static std::mutex mu;
+    static std::vector<int> done;  // devices with the attribute set
+    int dev = 0;
+    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    std::lock_guard<std::mutex> lock(mu);
+    bool have = false;
+    for (int d : done) have = have || d == dev;
+    if (!have) {
+      check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, PS::SMEM),
+                 "persistent Lanczos smem attr");
+      int per_sm = 0;
+      check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, PS::SMEM), "occupancy");
+      if (per_sm < 1) fail(RPM_E_UNSUPPORTED, "persistent Lanczos kernel does not fit on an SM");
+      done.push_back(dev);
+    }
+  }
+  const CUtensorMap map = basis_map<PS>(V_base, nslots, p.ld);
+  kern<<<sm_count(), kThreads, PS::SMEM, st>>>(map, p);
+  check_launch("k_lanczos_persistent");
+}
+
+using Launcher = void (*)(const PersistentLanczos&, const float2*, long long, cudaStream_t);
+
+Launcher pick(const CubePlan& plan, int* ltiles) {
+  if (!plan.fast) return nullptr;
+  const int l1 = plan.fl_n1, lh = plan.fl_nh, r1 = plan.fr_n1, rh = plan.fr_nh;
+  if (l1 == 2 && lh == 5 && r1 == 1 && rh == 6) {
+    if (ltiles) *ltiles = PShape<2, 5, 1, 6>::LT;
+    return launch_instance<2, 5, 1, 6>;
+  }
+  if (l1 == 2 && lh == 3 && r1 == 1 && rh == 4) {
+    if (ltiles) *ltiles = PShape<2, 3, 1, 4>::LT;
+    return launch_instance<2, 3, 1, 4>;
+  }
+  return nullptr;
+}
+
+}  // namespace
+
+int persistent_l_tiles(const CubePlan& plan) {
+  int lt = 0;
+  return pick(plan, &lt) ? lt : 0;
+}
+
+bool launch_lanczos_persistent(const PersistentLanczos& p, const CubePlan& plan, const float2* V_base, long long nslots,
+                               cudaStream_t stream) {
+  const Launcher fn = pick(plan, nullptr);
+  if (!fn) return false;
+  if (p.nb < 1 || p.m < 1 || p.gv < 1 || p.j0 < 0 || p.j1 <= p.j0 || p.j1 > p.m)
+    fail(RPM_E_INVALID, "persistent Lanczos: empty launch or bad iteration range");
+  if (p.part_stride < 3 * persistent_l_tiles(plan)) fail(RPM_E_INVALID, "persistent Lanczos: partial-sum stride");
+  auto aligned = [](const void* ptr) { return (reinterpret_cast<uintptr_t>(ptr) & 15u) == 0; };
+  if (!aligned(p.V) || !aligned(p.ya) || !aligned(V_base) || (p.ld & 1) || (p.vstride & 1))
+    fail(RPM_E_INVALID, "persistent Lanczos: basis and partials need 16-byte alignment");
+  fn(p, V_base, nslots, stream);
+  return true;
+}
+
+}  // namespace rpm
