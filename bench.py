@@ -41,15 +41,19 @@ GRID_US = 0.00125
 LIFETIME_US = 1.0
 YIELD_TOL = 1e-6  # singlet-yield error bar of the metric
 FALLBACK_HBM_GBS = 6650.0
+WORKLOAD = ("221,184-dim synthetic FAD-TrpH-shaped radical pair (2 e + 11 spin-1/2 + 3 spin-1), random-phase "
+            "trajectories to 5 us on the 0.00125-us grid (4001 points), singlet yield tau = 1 us, yield error <= 1e-6")
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline (oracle port), run in spawned worker processes
+# CPU baseline (oracle port): one spawned process per host core, each owning
+# one trajectory that it advances segment by segment
 # ---------------------------------------------------------------------------
-_CPU_STATE = {}
+def _cpu_worker_main(conn, seed: int, budget: float) -> None:
+    for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[var] = "1"
+    import numpy as np
 
-
-def _cpu_worker_init():
     import oracle
     from rpm_b200 import synthetic
 
@@ -57,50 +61,78 @@ def _cpu_worker_init():
     terms = full.terms(math.pi / 4, 0.0)
     h = oracle.CompiledFullPairHamiltonian(full.dimensions, [oracle.LocalTerm(t.axes, t.operator) for t in terms],
                                            left_axes=full.left_axes, right_axes=full.right_axes)
-    _CPU_STATE["h"] = h
-    _CPU_STATE["dims"] = full.dimensions
-
-
-def _cpu_worker_run(args):
-    seed, horizon = args
-    import numpy as np
-
-    import oracle
-    from rpm_b200 import synthetic
-
-    h = _CPU_STATE["h"]
-    psi = synthetic.random_phase_vectors(_CPU_STATE["dims"], 1, seed)[0]
-    times = np.arange(int(round(horizon / GRID_US)) + 1) * GRID_US
-    prop = oracle.AdaptiveLanczosPropagator(h, minimum_dimension=8, maximum_dimension=40,
-                                            state_error_budget=1e-10 * horizon / HORIZON_US)
-    t0 = time.perf_counter()
-    res = prop.propagate(psi, times, oracle.SingletPopulationObservable(_CPU_STATE["dims"]))
-    return time.perf_counter() - t0, res.stats.matvecs
+    observable = oracle.SingletPopulationObservable(full.dimensions)
+    psi = synthetic.random_phase_vectors(full.dimensions, 1, seed)[0]
+    conn.send("ready")
+    while True:
+        duration = conn.recv()
+        if duration is None:
+            break
+        # the state carries over from the previous segment (H is time independent);
+        # the budget is scaled by the segment's share of the 5-us horizon
+        times = np.arange(int(round(duration / GRID_US)) + 1) * GRID_US
+        prop = oracle.AdaptiveLanczosPropagator(h, minimum_dimension=8, maximum_dimension=40,
+                                                state_error_budget=budget * duration / HORIZON_US)
+        t0 = time.perf_counter()
+        res = prop.propagate(psi, times, observable)
+        psi = res.final_state
+        conn.send((time.perf_counter() - t0, int(res.stats.matvecs)))
+    conn.close()
 
 
 class CpuBaseline:
-    """The oracle's FP64 port on `workers` host processes (one BLAS thread each)."""
+    """The oracle's FP64 port (the reference's controller, Krylov 8-40) on
+    `workers` host processes with one BLAS thread each, every process
+    propagating its own trajectory of the benchmark system at theta = pi/4."""
 
-    def __init__(self, workers: int):
+    def __init__(self, workers: int, budget: float, seed0: int = 77):
         import multiprocessing as mp
 
-        for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
-            os.environ[var] = "1"
-        self.workers = workers
-        self.pool = mp.get_context("spawn").Pool(workers, initializer=_cpu_worker_init)
+        ctx = mp.get_context("spawn")
+        self.workers, self.budget = workers, budget
+        self.conns, self.procs = [], []
+        for k in range(workers):
+            parent, child = ctx.Pipe()
+            proc = ctx.Process(target=_cpu_worker_main, args=(child, seed0 + k, budget), daemon=True)
+            proc.start()
+            self.conns.append(parent)
+            self.procs.append(proc)
+        for c in self.conns:
+            if c.recv() != "ready":
+                raise RuntimeError("CPU baseline worker failed to start")
+        self.simulated_us = 0.0
+        self.matvecs = 0
 
-    def round(self, horizon: float, seed0: int):
-        """One round: every worker propagates one trajectory over `horizon` us."""
+    def segment(self, duration_us: float) -> float:
+        """Advance every worker's trajectory by `duration_us`; wall seconds."""
         t0 = time.perf_counter()
-        out = self.pool.map(_cpu_worker_run, [(seed0 + k, horizon) for k in range(self.workers)])
-        wall = time.perf_counter() - t0
-        per_traj = sum(o[0] for o in out) / len(out)
-        # trajectories/s over the full horizon, all workers in parallel
-        return self.workers / (wall * HORIZON_US / horizon), per_traj, wall
+        for c in self.conns:
+            c.send(float(duration_us))
+        out = [c.recv() for c in self.conns]
+        self.simulated_us += duration_us
+        self.matvecs += sum(o[1] for o in out)
+        return time.perf_counter() - t0
 
     def close(self):
-        self.pool.close()
-        self.pool.join()
+        for c in self.conns:
+            try:
+                c.send(None)
+            except OSError:
+                pass
+        for p in self.procs:
+            p.join(timeout=30)
+
+
+def extrapolation_record():
+    """The committed once-only validation of the prefix extrapolation
+    (oracle/cpu_extrapolation.json, written by oracle/cpu_extrapolation.py)."""
+    path = ROOT / "oracle" / "cpu_extrapolation.json"
+    try:
+        rec = json.loads(path.read_text())
+    except (OSError, ValueError):
+        return None
+    return {"source": "oracle/cpu_extrapolation.json", "host": rec.get("host"), "summary": rec.get("summary"),
+            "port_over_reference": rec.get("port_over_reference")}
 
 
 def cpu_workers() -> int:
@@ -188,29 +220,48 @@ def ncu_traffic_per_vector(fused: bool):
 # Arms
 # ---------------------------------------------------------------------------
 def reference_arm(args, rank: int, world: int) -> None:
+    """The reference's FP64 path (oracle port) on the host cores: every core
+    advances its own trajectory of the benchmark system; each step is one
+    segment of ``--ref-horizon / steps`` us (warm-up steps are further
+    segments), so the timed steps together cover a ``--ref-horizon``-us
+    prefix of every trajectory at the GPU arm's state-error budget (scaled by
+    the segment's share of the 5-us horizon).  Trajectories/s extrapolate the
+    simulated microseconds to 5-us trajectories; the committed validation
+    record gives the full-over-extrapolated time ratio and the port's speed
+    relative to the reference's own code."""
     if rank != 0:
         return
-    base = CpuBaseline(cpu_workers())
-    horizon = args.cpu_horizon
-    for k in range(args.warmup):
-        base.round(horizon, 1000 + 64 * k)
-    vals = []
-    t0 = time.perf_counter()
-    for k in range(args.steps):
-        v, _, _ = base.round(horizon, 5000 + 64 * k)
-        vals.append(v)
-    wall = time.perf_counter() - t0
+    from rpm_b200.autotune import budget_for_yield_tolerance
+
+    budget = args.budget if args.budget is not None else budget_for_yield_tolerance(YIELD_TOL)
+    base = CpuBaseline(cpu_workers(), budget)
+    seg = args.ref_horizon / args.steps
+    for _ in range(args.warmup):
+        base.segment(seg)
+    walls = []
+    mv0 = base.matvecs
+    for _ in range(args.steps):
+        walls.append(base.segment(seg))
     base.close()
-    value = sum(vals) / len(vals)
+    wall = sum(walls)
+    timed_us = seg * args.steps
+    value = base.workers * (timed_us / HORIZON_US) / wall
+    cpu = {"value": value, "unit": UNIT, "cores": base.workers, "kind": "port",
+           "why_port": "the reference is pure Python/NumPy and cannot travel to the GPU box; the port restates "
+                       "its FP64 path (oracle/rpm_oracle.py) and its speed relative to the reference's own code "
+                       "is in extrapolation.port_over_reference",
+           "sample": f"{base.workers} trajectories (one per core), each advanced {timed_us:g} us over {args.steps} "
+                     f"steps after {args.warmup} warm-up segments, budget {budget:g} (the GPU arm's), "
+                     f"extrapolated to 5 us",
+           "budget": budget, "prefix_us": timed_us, "matvecs": base.matvecs - mv0,
+           "extrapolation": extrapolation_record()}
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * wall / max(1, args.steps), "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": "plain FP64 Lanczos (Krylov 8-40, budget 1e-10) on the 221,184-dim synthetic "
-                               "radical pair, theta = pi/4, one trajectory per host core, extrapolated from a "
-                               f"{horizon} us prefix to 5 us"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": base.workers, "kind": "port",
-                         "sample": f"each step: {base.workers} trajectories x {horizon} us prefix, extrapolated"},
+        "config": {"workload": WORKLOAD, "state_error_budget": budget, "krylov": "adaptive 8-40 (reference controller)",
+                   "parallelism": f"one trajectory per host core x{base.workers}"},
+        "cpu_baseline": cpu,
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -348,14 +399,31 @@ def uneven_sample(args) -> dict:
             "rates_per_us": [1.0, 2.0]}
 
 
+def ncu_traffic_per_vector_iteration():
+    """DRAM bytes per vector and Lanczos iteration of the persistent kernel
+    from its committed ncu summary, or None."""
+    path = ROOT / "profiles" / "lanczos_persistent_c64.md"
+    try:
+        for line in path.read_text().splitlines():
+            if line.startswith("dram_bytes_per_vector_iteration:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+BENCH_TILES = (8, 16, 24, 48)  # trajectories per propagate call (divisors of the 48-trajectory step)
+
+
 def b200_arm(args, rank: int, world: int, dist) -> None:
     import numpy as np
     import torch
 
     import rpm_b200 as rb
     from rpm_b200 import synthetic
+    from rpm_b200.autotune import KRYLOV_RANGE, budget_for_yield_tolerance, tune
     from rpm_b200.batched import BatchedPropagator
-    from rpm_b200.distributed import gather_yields, max_over_ranks
+    from rpm_b200.distributed import gather_yields, max_over_ranks, rank_shard
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     torch.cuda.set_device(dev)
@@ -365,36 +433,48 @@ def b200_arm(args, rank: int, world: int, dist) -> None:
                                            right_axes=full.right_axes) for th, ph in dirs]
     n = full.dimension
     nvec = args.vectors
-    ntraj = args.orientations * nvec
-    seed = 1000 + rank
-    vecs = synthetic.random_phase_vectors(full.dimensions, nvec, seed)
-    states = np.stack([vecs[v] for k in range(args.orientations) for v in range(nvec)])
-    system_index = np.array([k for k in range(args.orientations) for _ in range(nvec)], dtype=np.int32)
+    per_rank = args.orientations * nvec
+    # The whole job is world x (orientations x vectors) trajectories, the same
+    # list on every rank; each rank propagates its cost-balanced shard of it.
+    job = world * per_rank
+    start, end = rank_shard([n] * job, dist)
+    ntraj = end - start
+    gids = np.arange(start, end)
+    system_index = ((gids % per_rank) // nvec).astype(np.int32)
+    states = np.stack([synthetic.random_phase_vectors(full.dimensions, 1, 1000 + int(g // per_rank) * 1000
+                                                      + int(g % nvec))[0] for g in gids])
     times = np.arange(int(round(args.horizon / GRID_US)) + 1) * GRID_US
     tuning = None
-    krylov, budget = args.krylov, args.budget
-    if krylov == "auto" or budget is None:
-        # Krylov dimension over the batched configuration's range 16-40 (tile
-        # fixed at this workload's batch), budget from the yield tolerance
-        from rpm_b200.autotune import KRYLOV_RANGE, budget_for_yield_tolerance, tune
-
-        if krylov == "auto":
-            tuning = tune(hams, list(states), system_index, horizon_us=0.25, yield_tolerance=YIELD_TOL,
-                          krylov_dimensions=KRYLOV_RANGE, tiles=(ntraj,))
-            krylov = tuning.krylov_dimension
-        if budget is None:
-            budget = budget_for_yield_tolerance(YIELD_TOL)
+    krylov, budget, reorth = args.krylov, args.budget, args.reorth_period
+    tile = ntraj
+    if budget is None:
+        budget = budget_for_yield_tolerance(YIELD_TOL)
+    if krylov == "auto":
+        # Krylov cap over the batched configuration's range 16-40, tile over
+        # divisors of the step's batch, reorthogonalisation none / every 16
+        # iterations; only candidates within the yield accuracy gate compete
+        tiles = tuple(t for t in BENCH_TILES if ntraj % t == 0) or (ntraj,)
+        tuning = tune(hams, list(states), system_index, horizon_us=0.25, full_horizon_us=args.horizon,
+                      yield_tolerance=YIELD_TOL, krylov_dimensions=KRYLOV_RANGE, tiles=tiles,
+                      reorth_periods=(0, 16), lanczos_kernel=args.lanczos)
+        krylov, tile, reorth = tuning.krylov_dimension, tuning.tile, tuning.reorth_period
     krylov = int(krylov)
-    bp = BatchedPropagator(hams, krylov_dimension=krylov, state_error_budget=budget)
+    bp = BatchedPropagator(hams, krylov_dimension=krylov, state_error_budget=budget, lanczos_kernel=args.lanczos,
+                           wavefront=args.wavefront, reorth_period=reorth)
     ld = bp.leading_dimension
     pristine = torch.zeros((ntraj, ld), dtype=torch.complex128, device=dev)
     pristine[:, :n].copy_(torch.from_numpy(states))
     work = torch.empty_like(pristine)
+    chunks = [(a, min(a + tile, ntraj)) for a in range(0, ntraj, tile)]
 
     def step():
         work.copy_(pristine)
-        values, _, stats = bp.propagate_device(work, times, system_index)
-        return values, stats
+        values, stats = [], []
+        for a, b in chunks:
+            v, _, st = bp.propagate_device(work[a:b], times, system_index[a:b])
+            values.append(v)
+            stats.extend(st)
+        return torch.cat(values), stats
 
     for _ in range(args.warmup):
         step()
@@ -421,7 +501,8 @@ def b200_arm(args, rank: int, world: int, dist) -> None:
     clock_info = clocks.stop()
     elapsed = max_over_ranks(t_start.elapsed_time(t_end) / 1e3, dist, dev)
     counters = bp.counters(reset=True)
-    value = args.steps * ntraj * world / elapsed
+    kind = bp.lanczos_kind()
+    value = args.steps * job / elapsed
     yields = bp.yields_device(times, values, LIFETIME_US)
     yields_all = gather_yields(yields, dist)  # the only cross-rank data: per-trajectory yields
     bad = [s.status for s in stats if s.status]
@@ -436,58 +517,78 @@ def b200_arm(args, rank: int, world: int, dist) -> None:
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
+    d2h = 0
     for _ in range(e2e_steps):
-        res = bp.propagate(host_states, times, system_index=system_index, lifetime_us=LIFETIME_US)
+        d2h = 0
+        for a, b in chunks:
+            res = bp.propagate(host_states[a:b], times, system_index=system_index[a:b], lifetime_us=LIFETIME_US)
+            d2h += res.observable_values.nbytes + res.state_error_estimates.nbytes + res.yields.nbytes
     e1.record()
     torch.cuda.synchronize()
     e2e_elapsed = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist, dev)
-    e2e_value = e2e_steps * ntraj * world / e2e_elapsed
+    e2e_value = e2e_steps * job / e2e_elapsed
     h2d = ntraj * n * 16
-    d2h = res.observable_values.nbytes + res.state_error_estimates.nbytes + res.yields.nbytes
 
     line = None
     if rank == 0:
-        # roofline of the dominant kernel pair, timed live on iteration 1 of
-        # every Krylov step: with the shape-specialised passes one fused
-        # Lanczos iteration (read w'_j and v_{j-1}, write v_j and w'_{j+1}:
-        # 32 N bytes per vector), else one H psi (read psi, write H psi: 16 N)
-        fused = bool(hams[0]._system.fast_hpsi)
+        # roofline of the dominant kernel, timed live (CUDA events inside the
+        # graph) on the first Krylov step of every propagate call: one
+        # persistent launch runs all m Lanczos iterations of `tile`
+        # trajectories, each iteration reading w'_j and v_{j-1} and writing v_j
+        # and w'_{j+1} (32 N bytes per vector); the per-iteration pass pair
+        # moves the same bytes
         peak, peak_src = measured_peak_hbm()
-        hpsi_s = counters["hpsi_ms"] / 1e3
-        alg_bytes = (32.0 if fused else 16.0) * n * ntraj
-        achieved = alg_bytes / hpsi_s / 1e9 if hpsi_s > 0 else None
-        per_vec = ncu_traffic_per_vector(fused)
-        kernel = ("fast_pass_r + fast_pass_l (one fused Lanczos iteration: complex64 H psi + Paige 3-term "
-                  "recurrence, all trajectories)" if fused else
-                  "cube_pass_l + cube_pass_r (complex64 H psi, one batched launch pair)")
+        iter_s = counters["hpsi_ms"] / 1e3
+        persistent = kind == "persistent"
+        iters = krylov if persistent else 1
+        alg_bytes = 32.0 * n * tile * iters
+        launch_s = iter_s * iters
+        achieved = alg_bytes / launch_s / 1e9 if launch_s > 0 else None
+        per_vec_iter = ncu_traffic_per_vector_iteration() if persistent else ncu_traffic_per_vector(True)
+        kernel = (f"k_lanczos_persistent<2,5,1,6> (all {krylov} Lanczos iterations of a Krylov step for {tile} "
+                  "trajectories: complex64 H psi + Paige 3-term recurrence, TMA-staged)" if persistent else
+                  "fast_pass_r + fast_pass_l (one fused Lanczos iteration, all trajectories)")
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak if achieved else None,
-                    "traffic": per_vec * ntraj if per_vec is not None else None,
+                    "traffic": per_vec_iter * tile * iters if per_vec_iter is not None else None,
+                    "traffic_source": ("profiles/lanczos_persistent_c64.md (ncu capture of this kernel; command "
+                                       "there), scaled to one launch" if persistent else
+                                       "profiles/lanczos_iteration_fused_c64.md"),
                     "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured" else "fallback",
-                    "kernel": kernel, "algorithmic_bytes": alg_bytes, "avg_launch_ms": counters["hpsi_ms"],
-                    "samples": counters["hpsi_samples"]}
-        # plain single-vector FP64 GPU path on trajectory 0 (same state and system)
+                    "kernel": kernel, "algorithmic_bytes": alg_bytes, "avg_launch_ms": launch_s * 1e3,
+                    "ms_per_lanczos_iteration": counters["hpsi_ms"], "samples": counters["hpsi_samples"]}
+        # plain single-vector FP64 GPU path (config 1's drop-in), one
+        # trajectory per orientation: its time, and the batched yield errors
         plain, y_err = None, None
         if not args.no_plain:
-            t0 = time.perf_counter()
-            ref = rb.AdaptiveLanczosPropagator(hams[0], minimum_dimension=8, maximum_dimension=40,
-                                               state_error_budget=1e-10).propagate(
-                states[0], times, rb.SingletPopulationObservable(full.dimensions))
-            torch.cuda.synchronize()
-            plain_s = time.perf_counter() - t0
-            y_plain = rb.integrate_yield(times, ref.observable_values, LIFETIME_US)
-            y_err = abs(float(yields[0].item()) - y_plain)
-            plain = {"value": 1.0 / plain_s, "unit": UNIT,
-                     "sample": f"1 trajectory (orientation 0, vector 0), {args.horizon:g} us",
-                     "matvecs": ref.stats.matvecs, "krylov": "8-40", "budget": 1e-10}
+            errs, secs, mvs = [], 0.0, 0
+            for k in range(min(args.plain_trajectories, args.orientations)):
+                b = k * nvec  # orientation k, vector 0
+                t0 = time.perf_counter()
+                ref = rb.AdaptiveLanczosPropagator(hams[system_index[b]], minimum_dimension=8, maximum_dimension=40,
+                                                   state_error_budget=1e-10).propagate(
+                    states[b], times, rb.SingletPopulationObservable(full.dimensions))
+                torch.cuda.synchronize()
+                secs += time.perf_counter() - t0
+                mvs += ref.stats.matvecs
+                y_plain = rb.integrate_yield(times, ref.observable_values, LIFETIME_US)
+                errs.append(abs(float(yields[b].item()) - y_plain))
+            errs = np.asarray(errs)
+            y_err = {"max": float(errs.max()), "rms": float(np.sqrt(np.mean(errs ** 2))), "trajectories": int(errs.size),
+                     "per_orientation": [float(e) for e in errs]}
+            plain = {"value": errs.size / secs, "unit": UNIT,
+                     "sample": f"{errs.size} trajectories (vector 0 of each orientation), {args.horizon:g} us",
+                     "matvecs": mvs, "krylov": "8-40", "budget": 1e-10}
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            base = CpuBaseline(cpu_workers())
-            cpu_value, per_traj, wall = base.round(args.cpu_horizon, 77)
+            base = CpuBaseline(cpu_workers(), budget)
+            wall = base.segment(args.cpu_horizon)
             base.close()
-            cpu = {"value": cpu_value, "unit": UNIT, "cores": base.workers, "kind": "port",
-                   "sample": f"{base.workers} trajectories x {args.cpu_horizon} us prefix (Krylov 8-40, budget "
-                             f"1e-10 scaled), extrapolated to 5 us; {per_traj:.1f} s each"}
+            cpu = {"value": base.workers * (args.cpu_horizon / HORIZON_US) / wall, "unit": UNIT,
+                   "cores": base.workers, "kind": "port",
+                   "sample": f"{base.workers} trajectories (one per core) x {args.cpu_horizon:g} us prefix (Krylov "
+                             f"8-40, budget {budget:g} scaled to the prefix), extrapolated to 5 us; {wall:.1f} s",
+                   "extrapolation": extrapolation_record()}
         adjoint = None
         if world == 1 and not args.no_adjoint:
             adjoint = adjoint_sample(full, dirs[0], dev)
@@ -495,17 +596,16 @@ def b200_arm(args, rank: int, world: int, dist) -> None:
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c64 H-psi/basis + f64 Krylov control", "data": "synthetic",
-            "config": {"workload": f"batched mixed-precision propagation, 221,184-dim synthetic FAD-TrpH-shaped radical "
-                                   f"pair (2 e + 11 spin-1/2 + 3 spin-1), {args.orientations} Fibonacci field "
-                                   f"orientations x {nvec} random-phase vectors per GPU per step, {args.horizon:g} us, "
-                                   f"0.00125-us grid ({len(times)} points), singlet yield tau = 1 us",
-                       "trajectories_per_step_per_gpu": ntraj, "krylov_dim": krylov,
-                       "krylov_choice": ("autotuned over " + str([t["krylov_dimension"] for t in tuning.trials])
-                                         if tuning else "fixed"),
-                       "state_error_budget": budget, "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (Krylov basis " f"{ntraj * (krylov + 1) * n * 8 / 1e9:.1f} GB)"},
-            "autotune": ({"trials": [{k: t[k] for k in ("krylov_dimension", "throughput") if k in t}
-                                     for t in tuning.trials], "horizon_us": 0.25} if tuning else None),
+            "config": {"workload": WORKLOAD, "batch": f"{args.orientations} Fibonacci field orientations x {nvec} "
+                                                      "random-phase vectors per GPU per step",
+                       "trajectories_per_step_per_gpu": per_rank, "krylov_dim": krylov, "tile": tile,
+                       "reorth_period": reorth, "lanczos_kernel": kind,
+                       "tuning": ("autotuned: Krylov " + str(list(KRYLOV_RANGE)) + ", tile, reorthogonalisation "
+                                  "(none / 16), accuracy-gated" if tuning else "fixed"),
+                       "state_error_budget": budget, "parallelism": f"replicas x{world} (cost-balanced shards)",
+                       "l2": "inputs larger than L2 (Krylov basis " f"{tile * (krylov + 1) * n * 8 / 1e9:.1f} GB)"},
+            "autotune": ({"trials": tuning.trials, "horizon_us": 0.25, "budget_scaled_to_prefix": True}
+                         if tuning else None),
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -534,9 +634,18 @@ def main() -> None:
     p.add_argument("--budget", type=float, default=None,
                    help="accumulated state-error budget (default: half the 1e-6 yield tolerance)")
     p.add_argument("--e2e-steps", type=int, default=2)
-    p.add_argument("--cpu-horizon", type=float, default=0.025, help="us of the CPU baseline sample")
+    p.add_argument("--lanczos", choices=("persistent", "passes"), default="persistent",
+                   help="Lanczos iterations of a Krylov step: one persistent launch, or two pass launches each")
+    p.add_argument("--wavefront", type=int, default=0, help="persistent kernel: vectors per wavefront group (0: 12)")
+    p.add_argument("--reorth-period", type=int, default=0,
+                   help="reorthogonalise the next Lanczos vector every this many iterations (0: never)")
+    p.add_argument("--cpu-horizon", type=float, default=0.05, help="us of the GPU arm's CPU baseline sample")
+    p.add_argument("--ref-horizon", type=float, default=0.25,
+                   help="reference arm: us of every host trajectory covered by the timed steps")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison trajectory")
+    p.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison trajectories")
+    p.add_argument("--plain-trajectories", type=int, default=12,
+                   help="plain FP64 trajectories (vector 0 of that many orientations) for the yield errors")
     p.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-gradient side measurement")
     p.add_argument("--uneven", action="store_true",
                    help="diagnostic: uneven sizes (864 / 13,824 / 221,184) with unequal rates, --horizon us")

@@ -1,26 +1,34 @@
-"""Autotuner of the batched propagator: Krylov dimension, trajectory tile and step budget.
+"""Autotuner of the batched propagator: Krylov dimension, trajectory tile,
+reorthogonalisation policy and step budget.
 
-The batched path (:class:`rpm_b200.batched.BatchedPropagator`) has three
-knobs whose best values depend on the systems and the GPU:
+The batched path (:class:`rpm_b200.batched.BatchedPropagator`) has knobs whose
+best values depend on the systems and the GPU:
 
 * the Krylov dimension m (cost per Krylov step grows about linearly in m,
   the step the embedded error estimate allows grows faster than m);
 * the trajectory tile, i.e. how many trajectories one batch carries (larger
-  tiles amortise the per-step controller, which runs one CTA per trajectory,
-  and fill the GPU; the Krylov basis costs ``tile * (m + 1) * ld * 8`` bytes);
+  tiles amortise the per-step controller and fill the GPU; the Krylov basis
+  costs ``tile * (m + 1) * ld * 8`` bytes);
+* the reorthogonalisation policy of the complex64 Lanczos recurrence: none
+  (Paige's three-term form) or periodic (every P iterations the next vector
+  is reorthogonalised against the whole basis, two classical Gram-Schmidt
+  passes; the reference reorthogonalises every iteration,
+  rpm_statevector_engine.py:675-676);
 * the state-error budget.  The reference's bound on the population error is
   ``2 eps + eps**2`` (rpm_statevector_engine.py:541-543), and a yield is a
   weighted average of populations with weights of total at most one, so a
   yield tolerance ``tol`` admits ``eps <= tol / 2``; the tuner never picks a
   looser budget.
 
-Each candidate runs the real batched propagation for a short prefix of the
-horizon (the Hamiltonian is time independent, so the cost per simulated
-microsecond is stationary) and is scored in trajectory-microseconds per
-second.  The Lanczos recurrence is Paige's three-term form without
-reorthogonalisation: the complex64 rounding floor of the basis, not loss of
-orthogonality, limits the yields (measured against the FP64 path), so no
-reorthogonalisation policy is offered.
+Each candidate runs the real batched propagation for a prefix of the
+horizon with the budget scaled by prefix / horizon, so that every Krylov step
+meets the same local tolerance as in the full run (the Hamiltonian is time
+independent, so the cost per simulated microsecond is stationary), and is
+scored in trajectory-microseconds per second.  A candidate is eligible only if
+its prefix yields agree with a tight-budget run of the same trajectories
+within ``accuracy * prefix / horizon`` (errors accumulate over the horizon):
+speed never buys accuracy.  Trial trajectories are drawn round-robin over the
+sample's shapes (system dimensions), so uneven batches are represented.
 """
 
 from __future__ import annotations
@@ -41,6 +49,7 @@ KRYLOV_RANGE = (16, 24, 32, 40)      # the batched configuration's Krylov cap ra
 # longer Krylov steps for the same per-step controller work.
 KRYLOV_EXTENDED = (16, 24, 32, 40, 48, 56, 64)
 TILE_RANGE = (8, 16, 32, 48, 64)     # trajectories per batch
+REORTH_POLICIES = (0, 16)            # reorthogonalisation period (0: none)
 
 
 @dataclass
@@ -49,12 +58,14 @@ class TuneResult:
     tile: int
     state_error_budget: float
     throughput: float                 # trajectory-us simulated per second at the chosen point
+    reorth_period: int = 0
     trials: list = field(default_factory=list)
 
     def propagator(self, hamiltonians, **kwargs) -> BatchedPropagator:
         """A BatchedPropagator configured with the tuned knobs."""
         return BatchedPropagator(hamiltonians, krylov_dimension=self.krylov_dimension,
-                                 state_error_budget=self.state_error_budget, **kwargs)
+                                 state_error_budget=self.state_error_budget, reorth_period=self.reorth_period,
+                                 **kwargs)
 
     def to_json(self) -> str:
         return json.dumps(asdict(self))
@@ -67,34 +78,69 @@ def budget_for_yield_tolerance(tolerance: float) -> float:
     return 0.5 * tolerance
 
 
-def _trial(hams, states, system_index, times, m: int, budget: float, repeats: int) -> float:
+def spread_selection(system_index: Sequence[int], shape_of: Sequence, count: int) -> np.ndarray:
+    """``count`` sample positions drawn round-robin over the shapes of the
+    sample (in order of first appearance), each shape's positions in order."""
+    idx = np.asarray(system_index)
+    groups: dict = {}
+    for pos, k in enumerate(idx):
+        groups.setdefault(shape_of[int(k)], []).append(pos)
+    queues = [list(v) for v in groups.values()]
+    out = []
+    while len(out) < min(count, idx.size):
+        for q in queues:
+            if q and len(out) < count:
+                out.append(q.pop(0))
+    return np.asarray(sorted(out), dtype=np.int64)
+
+
+def _run(hams, states, system_index, times, m, budget, reorth, repeats, lifetime, kernel):
+    """(best seconds, prefix yields) of one candidate."""
     torch = _torch()
-    bp = BatchedPropagator(hams, krylov_dimension=m, state_error_budget=budget)
-    psi0 = bp.load_states(states, system_index)
+    bp = BatchedPropagator(hams, krylov_dimension=m, state_error_budget=budget, reorth_period=reorth,
+                           lanczos_kernel=kernel)
+    order = bp.shape_order(system_index)
+    idx = np.asarray(system_index) if order is None else np.asarray(system_index)[order]
+    sts = states if order is None else [states[k] for k in order]
+    psi0 = bp.load_states(sts, idx)
     work = torch.empty_like(psi0)
     work.copy_(psi0)
-    bp.propagate_device(work, times, system_index)  # warm-up: graph capture, buffers
-    best = float("inf")
+    bp.propagate_device(work, times, idx)  # warm-up: graph capture, buffers
+    best, values = float("inf"), None
     for _ in range(repeats):
         work.copy_(psi0)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        bp.propagate_device(work, times, system_index)
+        values, _, stats = bp.propagate_device(work, times, idx)
         torch.cuda.synchronize()
         best = min(best, time.perf_counter() - t0)
-    return best
+        if any(s.status for s in stats):
+            return best, None
+    yields = bp.yields_device(times, values, lifetime).cpu().numpy()
+    if order is not None:
+        inverse = np.empty_like(order)
+        inverse[order] = np.arange(order.size)
+        yields = yields[inverse]
+    return best, yields
 
 
 def tune(hamiltonians: Sequence, states, system_index: Sequence[int], *, horizon_us: float = 0.25,
-         grid_us: float = 0.00125, yield_tolerance: float = 1e-6, krylov_dimensions: Sequence[int] = KRYLOV_RANGE,
-         tiles: Sequence[int] | None = None, repeats: int = 1, memory_fraction: float = 0.6,
+         full_horizon_us: float = 5.0, grid_us: float = 0.00125, yield_tolerance: float = 1e-6,
+         accuracy: float | None = None, krylov_dimensions: Sequence[int] = KRYLOV_RANGE,
+         tiles: Sequence[int] | None = None, reorth_periods: Sequence[int] = (0,), repeats: int = 1,
+         memory_fraction: float = 0.6, lifetime_us: float = 1.0, lanczos_kernel: str = "persistent",
          cache: str | Path | None = None) -> TuneResult:
-    """Pick (Krylov dimension, tile, budget) for trajectories ``states`` of ``hamiltonians``.
+    """Pick (Krylov dimension, tile, reorthogonalisation period, budget) for
+    trajectories ``states`` of ``hamiltonians``.
 
     ``states``/``system_index`` are a representative sample of the workload
-    (at least as many trajectories as the largest tile tried); the trial
-    propagates them over ``horizon_us``.  Tiles whose Krylov basis would need
-    more than ``memory_fraction`` of the free device memory are skipped.  With
+    (at least as many trajectories as the largest tile tried).  Each
+    candidate propagates ``tile`` of them, spread over the sample's shapes,
+    over ``horizon_us`` with the budget scaled to that prefix; it is eligible
+    when its prefix yields are within ``accuracy`` (default: half the yield
+    tolerance) x prefix / horizon of a run at a hundredth of the budget with
+    the largest Krylov dimension.  Tiles whose Krylov basis would need more
+    than ``memory_fraction`` of the free device memory are skipped.  With
     ``cache`` the result is stored in (and reused from) that JSON file, keyed
     by the systems' dimensions, the device name and the search space.
     """
@@ -104,9 +150,12 @@ def tune(hamiltonians: Sequence, states, system_index: Sequence[int], *, horizon
     if idx.size == 0:
         raise ValueError("at least one sample trajectory is required")
     budget = budget_for_yield_tolerance(yield_tolerance)
+    accuracy = 0.5 * yield_tolerance if accuracy is None else float(accuracy)
     tiles = tuple(sorted({t for t in (tiles or TILE_RANGE) if t <= idx.size} or {int(idx.size)}))
+    reorths = tuple(int(p) for p in reorth_periods)
     key = json.dumps({"dims": sorted({h.dimension for h in hams}), "device": torch.cuda.get_device_name(),
-                      "m": list(krylov_dimensions), "tiles": list(tiles), "budget": budget, "horizon": horizon_us})
+                      "m": list(krylov_dimensions), "tiles": list(tiles), "reorth": list(reorths), "budget": budget,
+                      "horizon": horizon_us, "full": full_horizon_us, "accuracy": accuracy})
     if cache is not None:
         path = Path(cache)
         if path.exists():
@@ -114,26 +163,41 @@ def tune(hamiltonians: Sequence, states, system_index: Sequence[int], *, horizon
             if key in stored:
                 return TuneResult(**stored[key])
     times = np.arange(int(round(horizon_us / grid_us)) + 1) * grid_us
+    frac = horizon_us / full_horizon_us
+    trial_budget = budget * frac
+    gate = accuracy * frac
     ld = max(h.dimension for h in hams)
+    shapes = [(tuple(h.dimensions), tuple(getattr(h, "left_axes", ()))) for h in hams]
+    # tight-budget reference yields of every trajectory any tile uses
+    pool = spread_selection(idx, shapes, max(tiles))
+    _, ref_y = _run(hams, [states[k] for k in pool], idx[pool], times, max(krylov_dimensions), trial_budget / 100.0,
+                    0, 1, lifetime_us, lanczos_kernel)
+    ref_of = {int(p): y for p, y in zip(pool, ref_y)}
     free, _ = torch.cuda.mem_get_info()
     trials = []
     best = None
     for m in krylov_dimensions:
-        for tile in tiles:
-            need = tile * (m + 1) * ld * 8 + tile * ld * 32
-            if need > memory_fraction * free:
-                trials.append({"krylov_dimension": m, "tile": tile, "skipped": "memory"})
-                continue
-            sel = np.arange(tile)
-            secs = _trial(hams, [states[k] for k in sel], idx[sel], times, m, budget, repeats)
-            rate = tile * horizon_us / secs
-            trials.append({"krylov_dimension": m, "tile": tile, "seconds": secs, "throughput": rate})
-            if best is None or rate > best[0]:
-                best = (rate, m, tile)
+        for reorth in reorths:
+            for tile in tiles:
+                trial = {"krylov_dimension": m, "tile": tile, "reorth_period": reorth}
+                need = tile * (m + 1) * ld * 8 + tile * ld * 32
+                if need > memory_fraction * free:
+                    trials.append({**trial, "skipped": "memory"})
+                    continue
+                sel = pool[spread_selection(idx[pool], shapes, tile)]
+                secs, ys = _run(hams, [states[k] for k in sel], idx[sel], times, m, trial_budget, reorth, repeats,
+                                lifetime_us, lanczos_kernel)
+                rate = tile * horizon_us / secs
+                err = float(np.max(np.abs(ys - np.array([ref_of[int(p)] for p in sel])))) if ys is not None else None
+                ok = err is not None and err <= gate
+                trials.append({**trial, "seconds": secs, "throughput": rate, "yield_err_prefix": err,
+                               "yield_err_per_horizon": None if err is None else err / frac, "accepted": ok})
+                if ok and (best is None or rate > best[0]):
+                    best = (rate, m, tile, reorth)
     if best is None:
-        raise RuntimeError("no autotuner candidate fits in device memory")
+        raise RuntimeError("no autotuner candidate fits in device memory and meets the accuracy gate")
     result = TuneResult(krylov_dimension=best[1], tile=best[2], state_error_budget=budget, throughput=best[0],
-                        trials=trials)
+                        reorth_period=best[3], trials=trials)
     if cache is not None:
         path = Path(cache)
         stored = json.loads(path.read_text()) if path.exists() else {}

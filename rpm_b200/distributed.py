@@ -81,3 +81,41 @@ def gather_yields(yields, dist, counts: Sequence[int] | None = None):
     parts = [torch.empty_like(padded) for _ in range(world)]
     dist.all_gather(parts, padded)
     return torch.cat([p[:k] for p, k in zip(parts, counts)])
+
+
+def rank_shard(dimensions: Sequence[int], dist, expected_matvecs: Sequence[float] | None = None) -> tuple[int, int]:
+    """This rank's contiguous [start, end) block of a trajectory list that
+    every rank builds identically (cost-balanced by :func:`shard_bounds`)."""
+    rank, world = (dist.get_rank(), dist.get_world_size()) if dist is not None and dist.is_initialized() else (0, 1)
+    return shard_bounds(trajectory_costs(dimensions, expected_matvecs), world)[rank]
+
+
+def propagate_sharded(propagator, states, system_index: Sequence[int], times_us, dist, *, lifetime_us: float,
+                      dimensions: Sequence[int] | None = None):
+    """Propagate this rank's shard of a trajectory list with a
+    :class:`~rpm_b200.batched.BatchedPropagator` and all-gather the yields.
+
+    ``states``/``system_index`` describe the whole job, identically on every
+    rank; ``dimensions`` (default: each trajectory's system dimension) drives
+    the cost balance.  Returns (this rank's BatchedResult or None when its
+    shard is empty, (start, end), all yields in trajectory order)."""
+    import torch
+
+    idx = np.asarray(system_index)
+    dims = (np.asarray([propagator.hamiltonians[int(k)].dimension for k in idx]) if dimensions is None
+            else np.asarray(dimensions))
+    start, end = rank_shard(dims, dist)
+    result = None
+    if end > start:
+        result = propagator.propagate([states[k] for k in range(start, end)], times_us, system_index=idx[start:end],
+                                      lifetime_us=lifetime_us)
+        mine = torch.as_tensor(result.yields, dtype=torch.float64)
+    else:
+        mine = torch.zeros(0, dtype=torch.float64)
+    if dist is not None and dist.is_initialized() and dist.get_backend() == "nccl":
+        mine = mine.cuda()
+    counts = None
+    if dist is not None and dist.is_initialized():
+        world = dist.get_world_size()
+        counts = [e - s for s, e in shard_bounds(trajectory_costs(dims), world)]
+    return result, (start, end), gather_yields(mine, dist, counts)

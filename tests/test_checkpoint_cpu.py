@@ -40,3 +40,17 @@ def test_cell_rejects_missing_keys_and_nonfinite(tmp_path):
     with pytest.raises(ValueError, match="Nonfinite"):
         checkpoint.read_cell(p)
     assert json.loads(str(np.load(p)["metadata_json"])) == {}
+
+
+def test_f14_digest_matches_the_reference_runner():
+    """configuration_hash of the full-size runner's cells, pinned to digests
+    that the reference's own Config(...).digest produced
+    (tests/golden/make_checkpoint_golden.py)."""
+    from conftest import GOLDEN
+
+    cases = json.loads((GOLDEN / "f14_digests.json").read_text())
+    assert len(cases) >= 4
+    for case in cases:
+        mine = json.loads(json.dumps(checkpoint.f14_stable_dict(**case["config"]), sort_keys=True))
+        assert mine == case["stable_dict"]
+        assert checkpoint.f14_digest(**case["config"]) == case["digest"]

@@ -59,3 +59,66 @@ def test_two_gloo_ranks_gather_and_max():
     for rank, allv, t in results:
         assert allv == [0.0, 1.0, 2.0, 10.0, 11.0]
         assert t == 2.5
+
+
+class _FakeHam:
+    def __init__(self, dimension):
+        self.dimension = dimension
+
+
+class _FakePropagator:
+    """Stands in for BatchedPropagator on CPU: the 'yield' of a trajectory is
+    its state's first entry, so the gather order can be checked."""
+
+    def __init__(self, dims):
+        self.hamiltonians = [_FakeHam(d) for d in dims]
+
+    def propagate(self, states, times, *, system_index, lifetime_us):
+        import numpy as np
+
+        class R:
+            pass
+
+        r = R()
+        r.yields = np.array([float(s[0]) for s in states])
+        return r
+
+
+def _shard_main(rank, world, port, out):
+    import numpy as np
+    import torch.distributed as dist
+
+    from rpm_b200.distributed import propagate_sharded, rank_shard
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        prop = _FakePropagator([221184, 13824, 864])
+        index = np.array([0] * 3 + [1] * 5 + [2] * 8)
+        states = [np.array([float(k)]) for k in range(index.size)]
+        span = rank_shard([prop.hamiltonians[k].dimension for k in index], dist)
+        _, got_span, yields = propagate_sharded(prop, states, index, [0.0, 1.0], dist, lifetime_us=1.0)
+        out.put((rank, span, got_span, yields.tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_propagate_cost_balanced_shards():
+    import torch.multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_shard_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    results = sorted(q.get(timeout=120) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (_, s0, g0, y0), (_, s1, g1, y1) = results
+    assert s0 == g0 and s1 == g1 and s0[0] == 0 and s0[1] == s1[0] and s1[1] == 16
+    # the three 221,184-dim trajectories outweigh the other thirteen: rank 0 gets
+    # the first two only, rank 1 the rest
+    assert s0 == (0, 2)
+    assert y0 == y1 == [float(k) for k in range(16)]
