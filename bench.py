@@ -425,8 +425,11 @@ def b200_arm(args, rank: int, world: int, dist) -> None:
     from rpm_b200.batched import BatchedPropagator
     from rpm_b200.distributed import gather_yields, max_over_ranks, rank_shard
 
+    from rpm_b200 import _lib
+
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     torch.cuda.set_device(dev)
+    _lib.call("rpm_set_persistent_warps", args.persistent_warps)
     full = synthetic.full_system()
     dirs = synthetic.fibonacci_sphere(args.orientations)
     hams = [rb.CompiledFullPairHamiltonian(full.dimensions, full.terms(th, ph), left_axes=full.left_axes,
@@ -637,6 +640,8 @@ def main() -> None:
     p.add_argument("--lanczos", choices=("persistent", "passes"), default="persistent",
                    help="Lanczos iterations of a Krylov step: one persistent launch, or two pass launches each")
     p.add_argument("--wavefront", type=int, default=0, help="persistent kernel: vectors per wavefront group (0: 12)")
+    p.add_argument("--persistent-warps", type=int, choices=(8, 12), default=12,
+                   help="persistent kernel: consumer warps per CTA")
     p.add_argument("--reorth-period", type=int, default=0,
                    help="reorthogonalise the next Lanczos vector every this many iterations (0: never)")
     p.add_argument("--cpu-horizon", type=float, default=0.05, help="us of the GPU arm's CPU baseline sample")

@@ -25,10 +25,12 @@
 // and stages it with the Tensor Memory Accelerator into one of two shared-
 // memory stages (mbarrier transaction counts): pass-R rows by bulk copies into
 // padded rows, pass-L columns by 5-D tensor copies, the coefficient table by a
-// bulk copy.  Eight consumer warps compute the other stage meanwhile.
+// bulk copy.  Twelve (or eight) consumer warps compute the other stage
+// meanwhile.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -42,10 +44,8 @@ namespace {
 
 using namespace fastpass;
 
-constexpr int kConsumerWarps = 8;
-constexpr int kConsumers = kConsumerWarps * 32;
-constexpr int kThreads = kConsumers + 32;        // + one producer warp
 constexpr long long kWaitCycles = 4000000000LL;  // about 2 s at 1.965 GHz
+constexpr int kTabCache = 256;                   // vectors whose table pointers are cached in shared memory
 
 constexpr int align128c(int b) { return (b + 127) & ~127; }
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
@@ -121,16 +121,18 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 }
 // Barrier over the consumer warps only (the producer warp never joins it);
 // returns the AND of `ok` over them.
+template <int NC>
 __device__ __forceinline__ bool consumers_and(bool ok) {
   unsigned r;
   asm volatile(
       "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.and.pred q, 1, %2, p;\n selp.u32 %0, 1, 0, q;\n}\n"
       : "=r"(r)
-      : "r"((unsigned)ok), "r"(kConsumers)
+      : "r"((unsigned)ok), "n"(NC)
       : "memory");
   return r != 0;
 }
-__device__ __forceinline__ void consumers_sync() { asm volatile("bar.sync 1, %0;\n" ::"r"(kConsumers) : "memory"); }
+template <int NC>
+__device__ __forceinline__ void consumers_sync() { asm volatile("bar.sync 1, %0;\n" ::"n"(NC) : "memory"); }
 
 // Wait until *p >= need (acquire); false after the time limit or a raised status.
 __device__ bool wait_progress(const int* p, int need, int* status) {
@@ -213,9 +215,18 @@ __device__ __forceinline__ Item decode(long long idx, int mseg, int nb, int gv) 
   return it;
 }
 
-template <int N1L, int NHL, int N1R, int NHR>
-__global__ void __launch_bounds__(kThreads, 1)
+// CW consumer warps + one producer warp per CTA, one CTA per SM: the
+// register cap is the largest multiple of 8 that lets CW + 1 warps fit the
+// SM's 65,536 registers.
+template <int CW>
+struct PRegs {
+  static constexpr int value = (65536 / ((CW + 1) * 32)) / 8 * 8 > 255 ? 255 : (65536 / ((CW + 1) * 32)) / 8 * 8;
+};
+template <int N1L, int NHL, int N1R, int NHR, int CW>
+__global__ void __maxnreg__(PRegs<CW>::value)
     k_lanczos_persistent(const __grid_constant__ CUtensorMap vmap, PersistentLanczos p) {
+  constexpr int kConsumerWarps = CW;
+  constexpr int kConsumers = CW * 32;
   using PS = PShape<N1L, NHL, N1R, NHR>;
   using PR = typename PS::PR;
   using PL = typename PS::PL;
@@ -227,6 +238,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   __shared__ __align__(8) unsigned long long full_bar[2], empty_bar[2];
   __shared__ Item meta[2];
   __shared__ double red[kConsumerWarps][3];
+  __shared__ const float2* tab_ptr[2][kTabCache];  // per vector: pass-R / pass-L coefficient tables
   auto stage_tab = [&](int s) { return reinterpret_cast<float2*>(base + s * PS::STAGE); };
   auto stage_orec = [&](int s) { return reinterpret_cast<ORec<float2>*>(base + s * PS::STAGE + PS::TAB_BYTES); };
   auto stage_tile = [&](int s) {
@@ -239,6 +251,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
+  for (int b = threadIdx.x; b < min(p.nb, kTabCache); b += blockDim.x) {
+    const CubeView<float2>* v = p.views + (p.sys_of ? p.sys_of[b] : 0);
+    tab_ptr[0][b] = v->tabR;
+    tab_ptr[1][b] = v->tabL;
+  }
   __syncthreads();
   const int mseg = p.j1 - p.j0;
   const long long total = (long long)mseg * p.nb * PS::PT;
@@ -246,16 +263,22 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   if (warp == kConsumerWarps) {
     // ----------------------------- producer -----------------------------
-    // per stage: the last use armed (copies, skip or end) and whether it got copies
+    // per stage: the last use armed (copies or end) and whether it got copies
     long long armed_use[2] = {-1, -1};
     bool armed_copies[2] = {false, false};
+    // the dequeue runs one item ahead, so its latency overlaps the wait for a free stage
+    long long next_idx = 0;
+    if (lane == 0) next_idx = atomicAdd(p.work, 1u);
     for (long long it = 0;; ++it) {
       const int s = (int)(it & 1);
       const long long use = it >> 1;
       bool ok = true;
-      if (use >= 1 && lane == 0) ok = mbar_wait(&empty_bar[s], (unsigned)((use - 1) & 1), p.status);
       long long idx = 0;
-      if (lane == 0 && ok) idx = atomicAdd(p.work, 1u);
+      if (lane == 0) {
+        idx = next_idx;
+        if (use >= 1) ok = mbar_wait(&empty_bar[s], (unsigned)((use - 1) & 1), p.status);
+        if (ok && idx < total) next_idx = atomicAdd(p.work, 1u);
+      }
       ok = __shfl_sync(0xffffffffu, ok, 0);
       idx = __shfl_sync(0xffffffffu, idx, 0);
       Item m{};
@@ -266,26 +289,33 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (lane == 0) {
           const int need = m.kind == 0 ? 2 * m.j : 2 * m.j + 1;
           if (need > 0) ok = wait_progress(p.prog + m.b, need, p.status);
-          m.skip = ok ? *reinterpret_cast<volatile int*>(p.skip + (long long)m.b * p.istride) : 1;
         }
         ok = __shfl_sync(0xffffffffu, ok, 0);
-        m.skip = __shfl_sync(0xffffffffu, m.skip, 0);
         if (!ok) m.kind = -1;
       }
       armed_use[s] = use;
-      armed_copies[s] = !(m.kind < 0 || m.skip);
-      if (m.kind < 0 || m.skip) {
+      armed_copies[s] = m.kind >= 0;
+      if (m.kind < 0) {
         if (lane == 0) {
           meta[s] = m;
           mbar_arrive(&full_bar[s]);
         }
         __syncwarp();
-        if (m.kind < 0) break;
-        continue;
+        break;
       }
-      // stage the item's data
+      // stage the item's data (also for a vector that stopped: the consumers
+      // read its skip flag and leave the staged data unused)
       fence_proxy_async();
-      const CubeView<float2>* view = p.views + (p.sys_of ? p.sys_of[m.b] : 0);
+      const float2* tabR;
+      const float2* tabL;
+      if (m.b < kTabCache) {
+        tabR = tab_ptr[0][m.b];
+        tabL = tab_ptr[1][m.b];
+      } else {
+        const CubeView<float2>* view = p.views + (p.sys_of ? p.sys_of[m.b] : 0);
+        tabR = view->tabR;
+        tabL = view->tabL;
+      }
       const float2* vj = p.V + (long long)m.b * p.vstride + (long long)m.j * p.ld;
       float2* tile = stage_tile(s);
       if (m.kind == 0) {
@@ -298,7 +328,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           mbar_arrive_expect_tx(&full_bar[s], bytes);
         }
         __syncwarp();
-        if (lane == 0) bulk_g2s(stage_tab(s), view->tabR, PS::SR::NTAB * 8, &full_bar[s]);
+        if (lane == 0) bulk_g2s(stage_tab(s), tabR, PS::SR::NTAB * 8, &full_bar[s]);
         const int rr = lane & 15, which = lane >> 4;
         if (rr < rows && (which == 0 || prev)) {
           const float2* src = which == 0 ? vj : vj - p.ld;
@@ -316,7 +346,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           mbar_arrive_expect_tx(&full_bar[s], bytes);
         }
         __syncwarp();
-        if (lane == 0) bulk_g2s(stage_tab(s), view->tabL, PS::SL::NTAB * 8, &full_bar[s]);
+        if (lane == 0) bulk_g2s(stage_tab(s), tabL, PS::SL::NTAB * 8, &full_bar[s]);
         if (lane < 2 * PS::LSPLIT) {
           const int ea = lane / PS::LSPLIT, part = lane % PS::LSPLIT;
           const long long slot = p.slot0 + (long long)m.b * (p.m + 1) + m.j;
@@ -340,10 +370,14 @@ __global__ void __launch_bounds__(kThreads, 1)
   for (long long it = 0;; ++it) {
     const int s = (int)(it & 1);
     const unsigned parity = (unsigned)((it >> 1) & 1);
-    const bool ok = consumers_and(mbar_wait(&full_bar[s], parity, p.status));
+    const bool ok = consumers_and<kConsumers>(mbar_wait(&full_bar[s], parity, p.status));
     if (!ok) break;
-    const Item m = meta[s];
+    Item m = meta[s];
     if (m.kind < 0) break;
+    // a vector stopped by a breakdown (or finished before this Krylov step)
+    // keeps its counters moving but does no arithmetic; the flag was set
+    // before the progress this item waited for
+    m.skip = *reinterpret_cast<volatile int*>(p.skip + (long long)m.b * p.istride);
     float2* tab = stage_tab(s);
     ORec<float2>* orec = stage_orec(s);
     float2* tile = stage_tile(s);
@@ -384,12 +418,12 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
         }
         build_orec<float2, typename PS::SR, PS::SR::K - 2, 4>(tab, orec, PR::NO, tid, kConsumers);
-        consumers_sync();
+        consumers_sync<kConsumers>();
         r_tile_math<float2, N1R, NHR>(tab, orec, tile, ptile, rows, row0, HL, QUARTER, yb, 1.0f, bprev, prev, warp,
                                       kConsumerWarps);
       } else {
         build_orec<float2, typename PS::SL, PS::SL::K - 3, 8>(tab, orec, PL::NO, tid, kConsumers);
-        consumers_sync();
+        consumers_sync<kConsumers>();
         l_tile_math<float2, N1L, NHL>(tab, orec, tile, view, m.tile * 8, QUARTER, yb, vj + p.ld, 1.0f,
                                       m.j < p.m - 1, warp, kConsumerWarps, dot, nw, nv);
         dot = warp_sum_d(dot);
@@ -401,13 +435,15 @@ __global__ void __launch_bounds__(kThreads, 1)
           red[warp][2] = nv;
         }
       }
-      // this thread's global writes before the tile is counted, for generic
-      // and tensor-copy readers on other SMs
+    }
+    // the CTA barrier orders every consumer's global writes before thread 0's
+    // device-scope fence and counter update (the grid-barrier pattern);
+    // readers on other SMs acquire the progress counter, and their producer
+    // fences the async proxy before its tensor copies
+    consumers_sync<kConsumers>();
+    if (tid == 0) {
       __threadfence();
       fence_proxy_async();
-    }
-    consumers_sync();
-    if (tid == 0) {
       const int ntiles = m.kind == 0 ? PS::RT : PS::LT;
       if (m.kind == 1 && !m.skip) {
         double t0 = 0.0, t1 = 0.0, t2 = 0.0;
@@ -496,11 +532,12 @@ CUtensorMap basis_map(const float2* V, long long nslots, long long ld) {
   return map;
 }
 
-template <int N1L, int NHL, int N1R, int NHR>
+template <int N1L, int NHL, int N1R, int NHR, int CW>
 void launch_instance(const PersistentLanczos& p, const float2* V_base, long long nslots, cudaStream_t st) {
   using PS = PShape<N1L, NHL, N1R, NHR>;
   static_assert(PS::SMEM <= 227 * 1024, "persistent Lanczos stages exceed shared memory");
-  auto kern = k_lanczos_persistent<N1L, NHL, N1R, NHR>;
+  constexpr int kThreads = CW * 32 + 32;
+  auto kern = k_lanczos_persistent<N1L, NHL, N1R, NHR, CW>;
   {
     static std::mutex mu;
     static std::vector<int> done;  // devices with the attribute set
@@ -525,16 +562,21 @@ void launch_instance(const PersistentLanczos& p, const float2* V_base, long long
 
 using Launcher = void (*)(const PersistentLanczos&, const float2*, long long, cudaStream_t);
 
+// Consumer warps per CTA: 12 (two pass-R and three pass-L warp tasks per
+// warp on the full system) or 8; set by rpm_set_persistent_warps.
+std::atomic<int> g_consumer_warps{12};
+
 Launcher pick(const CubePlan& plan, int* ltiles) {
   if (!plan.fast) return nullptr;
   const int l1 = plan.fl_n1, lh = plan.fl_nh, r1 = plan.fr_n1, rh = plan.fr_nh;
+  const bool w12 = g_consumer_warps.load(std::memory_order_relaxed) == 12;
   if (l1 == 2 && lh == 5 && r1 == 1 && rh == 6) {
     if (ltiles) *ltiles = PShape<2, 5, 1, 6>::LT;
-    return launch_instance<2, 5, 1, 6>;
+    return w12 ? launch_instance<2, 5, 1, 6, 12> : launch_instance<2, 5, 1, 6, 8>;
   }
   if (l1 == 2 && lh == 3 && r1 == 1 && rh == 4) {
     if (ltiles) *ltiles = PShape<2, 3, 1, 4>::LT;
-    return launch_instance<2, 3, 1, 4>;
+    return w12 ? launch_instance<2, 3, 1, 4, 12> : launch_instance<2, 3, 1, 4, 8>;
   }
   return nullptr;
 }
@@ -561,3 +603,10 @@ bool launch_lanczos_persistent(const PersistentLanczos& p, const CubePlan& plan,
 }
 
 }  // namespace rpm
+
+extern "C" int rpm_set_persistent_warps(int consumer_warps) {
+  return rpm::guarded([&] {
+    if (consumer_warps != 8 && consumer_warps != 12) rpm::fail(RPM_E_INVALID, "consumer warps must be 8 or 12");
+    rpm::g_consumer_warps.store(consumer_warps, std::memory_order_relaxed);
+  });
+}

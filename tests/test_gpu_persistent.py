@@ -34,11 +34,14 @@ def _plain_yield(rb, h, psi, times, dims):
     return ref.observable_values, rb.integrate_yield(times, ref.observable_values, 1.0)
 
 
+@pytest.mark.parametrize("warps", [12, 8])
 @pytest.mark.parametrize("which,nvec,wavefront,krylov", [("prefix", 7, 3, 16), ("full", 6, 12, 16),
                                                          ("full", 5, 2, 24)])
-def test_persistent_matches_pass_launches(which, nvec, wavefront, krylov):
-    from rpm_b200 import synthetic
+def test_persistent_matches_pass_launches(which, nvec, wavefront, krylov, warps):
+    from rpm_b200 import _lib, synthetic
     from rpm_b200.batched import BatchedPropagator
+
+    _lib.call("rpm_set_persistent_warps", warps)
 
     sub, hams = _systems(which, 2)
     states = synthetic.random_phase_vectors(sub.dimensions, nvec, 11)
@@ -51,6 +54,7 @@ def test_persistent_matches_pass_launches(which, nvec, wavefront, krylov):
         out[kind] = bp.propagate(list(states), times, system_index=index, lifetime_us=1.0)
         assert bp.lanczos_kind() == kind
         assert not np.any(out[kind].status)
+    _lib.call("rpm_set_persistent_warps", 12)
     a, b = out["persistent"], out["passes"]
     assert np.max(np.abs(a.observable_values - b.observable_values)) < SAME_TOL
     assert np.max(np.abs(a.yields - b.yields)) < SAME_TOL
