@@ -25,8 +25,8 @@
 // and stages it with the Tensor Memory Accelerator into one of two shared-
 // memory stages (mbarrier transaction counts): pass-R rows by bulk copies into
 // padded rows, pass-L columns by 5-D tensor copies, the coefficient table by a
-// bulk copy.  Twelve (or eight) consumer warps compute the other stage
-// meanwhile.
+// bulk copy.  Eleven consumer warps (8 or 12 selectable) compute the other
+// stage meanwhile.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -215,12 +215,15 @@ __device__ __forceinline__ Item decode(long long idx, int mseg, int nb, int gv) 
   return it;
 }
 
-// CW consumer warps + one producer warp per CTA, one CTA per SM: the
-// register cap is the largest multiple of 8 that lets CW + 1 warps fit the
-// SM's 65,536 registers.
+// CW consumer warps + one producer warp per CTA, one CTA per SM.  Registers
+// are allocated per SM sub-partition (4 per SM, 16,384 registers each, warps
+// assigned round-robin), so the cap is the largest multiple of 8 that fits
+// ceil((CW + 1) / 4) warps into one sub-partition.
 template <int CW>
 struct PRegs {
-  static constexpr int value = (65536 / ((CW + 1) * 32)) / 8 * 8 > 255 ? 255 : (65536 / ((CW + 1) * 32)) / 8 * 8;
+  static constexpr int per_part = (CW + 1 + 3) / 4;
+  static constexpr int raw = 16384 / (per_part * 32) / 8 * 8;
+  static constexpr int value = raw > 255 ? 255 : raw;
 };
 template <int N1L, int NHL, int N1R, int NHR, int CW>
 __global__ void __maxnreg__(PRegs<CW>::value)
@@ -562,21 +565,31 @@ void launch_instance(const PersistentLanczos& p, const float2* V_base, long long
 
 using Launcher = void (*)(const PersistentLanczos&, const float2*, long long, cudaStream_t);
 
-// Consumer warps per CTA: 12 (two pass-R and three pass-L warp tasks per
-// warp on the full system) or 8; set by rpm_set_persistent_warps.
-std::atomic<int> g_consumer_warps{12};
+// Consumer warps per CTA (8, 11 or 12; set by rpm_set_persistent_warps):
+// 8 and 11 keep 168 registers per thread, 12 (two pass-R and three pass-L
+// warp tasks per warp on the full system) caps them at 128.
+std::atomic<int> g_consumer_warps{11};
+
+template <int N1L, int NHL, int N1R, int NHR>
+Launcher by_warps(int warps) {
+  switch (warps) {
+    case 8: return launch_instance<N1L, NHL, N1R, NHR, 8>;
+    case 12: return launch_instance<N1L, NHL, N1R, NHR, 12>;
+    default: return launch_instance<N1L, NHL, N1R, NHR, 11>;
+  }
+}
 
 Launcher pick(const CubePlan& plan, int* ltiles) {
   if (!plan.fast) return nullptr;
   const int l1 = plan.fl_n1, lh = plan.fl_nh, r1 = plan.fr_n1, rh = plan.fr_nh;
-  const bool w12 = g_consumer_warps.load(std::memory_order_relaxed) == 12;
+  const int warps = g_consumer_warps.load(std::memory_order_relaxed);
   if (l1 == 2 && lh == 5 && r1 == 1 && rh == 6) {
     if (ltiles) *ltiles = PShape<2, 5, 1, 6>::LT;
-    return w12 ? launch_instance<2, 5, 1, 6, 12> : launch_instance<2, 5, 1, 6, 8>;
+    return by_warps<2, 5, 1, 6>(warps);
   }
   if (l1 == 2 && lh == 3 && r1 == 1 && rh == 4) {
     if (ltiles) *ltiles = PShape<2, 3, 1, 4>::LT;
-    return w12 ? launch_instance<2, 3, 1, 4, 12> : launch_instance<2, 3, 1, 4, 8>;
+    return by_warps<2, 3, 1, 4>(warps);
   }
   return nullptr;
 }
@@ -606,7 +619,8 @@ bool launch_lanczos_persistent(const PersistentLanczos& p, const CubePlan& plan,
 
 extern "C" int rpm_set_persistent_warps(int consumer_warps) {
   return rpm::guarded([&] {
-    if (consumer_warps != 8 && consumer_warps != 12) rpm::fail(RPM_E_INVALID, "consumer warps must be 8 or 12");
+    if (consumer_warps != 8 && consumer_warps != 11 && consumer_warps != 12)
+      rpm::fail(RPM_E_INVALID, "consumer warps must be 8, 11 or 12");
     rpm::g_consumer_warps.store(consumer_warps, std::memory_order_relaxed);
   });
 }
