@@ -640,7 +640,7 @@ def main() -> None:
     p.add_argument("--lanczos", choices=("persistent", "passes"), default="persistent",
                    help="Lanczos iterations of a Krylov step: one persistent launch, or two pass launches each")
     p.add_argument("--wavefront", type=int, default=0, help="persistent kernel: vectors per wavefront group (0: 12)")
-    p.add_argument("--persistent-warps", type=int, choices=(8, 11, 12), default=11,
+    p.add_argument("--persistent-warps", type=int, choices=(8, 10), default=8,
                    help="persistent kernel: consumer warps per CTA")
     p.add_argument("--reorth-period", type=int, default=0,
                    help="reorthogonalise the next Lanczos vector every this many iterations (0: never)")

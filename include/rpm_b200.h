@@ -303,9 +303,8 @@ int rpm_batch_counters(rpm_batch* batch, int reset, long long* kernel_launches, 
  * (per segment between reorthogonalisations), 1 shape-specialised pass pairs
  * per iteration, 2 general cube kernels (or Arnoldi). */
 int rpm_batch_lanczos_kind(const rpm_batch* batch, int* kind);
-/* Consumer warps per CTA of the persistent Lanczos kernel, 8, 11 or 12
- * (default 11); a tuning knob for measurements, no counterpart in the
- * reference. */
+/* Consumer warps per CTA of the persistent Lanczos kernel, 8 or 10 (default
+ * 8); a tuning knob for measurements, no counterpart in the reference. */
 int rpm_set_persistent_warps(int consumer_warps);
 /* Replace the configured state-error budget for later propagate calls (the
  * knob ENG:620-649 exposes as a mutable attribute). */

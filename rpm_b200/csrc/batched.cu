@@ -1218,6 +1218,7 @@ struct rpm_batch {
   struct ShapeGroup {
     int b0, nb;
     rpm::CubePlan plan;
+    bool records;  // every member carries the outer-index records of the persistent kernel
   };
   std::vector<ShapeGroup> groups;
   int dot_stride = 1;  // partial-sum slots per trajectory
@@ -1394,7 +1395,7 @@ static void record_step(rpm_batch* Bh, const BatchDev& B, const Layout& L, cudaS
   std::vector<char> gpers(Bh->groups.size());
   int npers = 0;
   for (size_t g = 0; g < Bh->groups.size(); ++g) {
-    gpers[g] = Bh->cfg.lanczos_kernel == RPM_LANCZOS_PERSISTENT && gfused[g] &&
+    gpers[g] = Bh->cfg.lanczos_kernel == RPM_LANCZOS_PERSISTENT && gfused[g] && Bh->groups[g].records &&
                persistent_l_tiles(Bh->groups[g].plan) > 0;
     npers += gpers[g];
   }
@@ -1547,7 +1548,9 @@ static void run_batch(rpm_batch* Bh, int ntraj, const int* sys_of, void* psi, co
       rpm_system* sk = Bh->systems[sys_of[k]];
       if (std::find(members.begin(), members.end(), sk) == members.end()) members.push_back(sk);
     }
-    Bh->groups.push_back({b, e - b, cube_plan(members.data(), (int)members.size())});
+    bool records = true;
+    for (const rpm_system* sk : members) records = records && sk->cube32.orecR && sk->cube32.orecL;
+    Bh->groups.push_back({b, e - b, cube_plan(members.data(), (int)members.size()), records});
     b = e;
   }
   // partial-sum slots per trajectory: general pass R (grid.x <= nl) or fused pass L (3 per block)

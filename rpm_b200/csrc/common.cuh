@@ -178,6 +178,13 @@ struct CubeView {
   const int* offr;
   int nl, nr, half_l, half_r;
   int inner_l, inner_r;  // usable trailing spin-1/2 digits per side
+  // complex64 views of shapes with shape-specialised passes: per outer index
+  // the merged diagonal / electron-flip records of pass R (outer digits
+  // 0..K-3 of the right radical) and pass L (0..K-4 of the left), laid out as
+  // {float d[2]; float2 f[2]} (24 bytes) and padded to 16 bytes; else null
+  const void* orecR;
+  const void* orecL;
+  int orec_bytes_r, orec_bytes_l;
 };
 
 }  // namespace rpm

@@ -24,9 +24,10 @@
 // Inside a CTA one producer warp dequeues, waits for the item's dependencies
 // and stages it with the Tensor Memory Accelerator into one of two shared-
 // memory stages (mbarrier transaction counts): pass-R rows by bulk copies into
-// padded rows, pass-L columns by 5-D tensor copies, the coefficient table by a
-// bulk copy.  Eleven consumer warps (8 or 12 selectable) compute the other
-// stage meanwhile.
+// padded rows, pass-L columns by 5-D tensor copies, the coefficient table and
+// the outer-index records by bulk copies.  Eight consumer warps (10
+// selectable) compute the other stage meanwhile, and a finisher warp does the
+// device-scope bookkeeping of finished tiles.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -119,21 +120,6 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
 __device__ __forceinline__ void st_release(int* p, int v) {
   asm volatile("st.release.gpu.global.b32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
 }
-// Barrier over the consumer warps only (the producer warp never joins it);
-// returns the AND of `ok` over them.
-template <int NC>
-__device__ __forceinline__ bool consumers_and(bool ok) {
-  unsigned r;
-  asm volatile(
-      "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.and.pred q, 1, %2, p;\n selp.u32 %0, 1, 0, q;\n}\n"
-      : "=r"(r)
-      : "r"((unsigned)ok), "n"(NC)
-      : "memory");
-  return r != 0;
-}
-template <int NC>
-__device__ __forceinline__ void consumers_sync() { asm volatile("bar.sync 1, %0;\n" ::"n"(NC) : "memory"); }
-
 // Wait until *p >= need (acquire); false after the time limit or a raised status.
 __device__ bool wait_progress(const int* p, int need, int* status) {
   const long long t0 = clock64();
@@ -215,42 +201,71 @@ __device__ __forceinline__ Item decode(long long idx, int mseg, int nb, int gv) 
   return it;
 }
 
-// CW consumer warps + one producer warp per CTA, one CTA per SM.  Registers
-// are allocated per SM sub-partition (4 per SM, 16,384 registers each, warps
-// assigned round-robin), so the cap is the largest multiple of 8 that fits
-// ceil((CW + 1) / 4) warps into one sub-partition.
+// CW consumer warps, one producer warp and one finisher warp per CTA, one
+// CTA per SM.  Registers are allocated per SM sub-partition (4 per SM,
+// 16,384 registers each, warps assigned round-robin), so the cap is the
+// largest multiple of 8 that fits ceil((CW + 2) / 4) warps into one
+// sub-partition.
 template <int CW>
 struct PRegs {
-  static constexpr int per_part = (CW + 1 + 3) / 4;
+  static constexpr int per_part = (CW + 2 + 3) / 4;
   static constexpr int raw = 16384 / (per_part * 32) / 8 * 8;
   static constexpr int value = raw > 255 ? 255 : raw;
 };
+
+// Per stage (two stages), the item moves through three roles:
+//   producer  -- dequeues, waits for the item's dependency, stages tiles,
+//                table and outer records by TMA, completes full[s];
+//   consumers -- wait full[s], compute their warp tasks (the pass-R combine
+//                of v_j is shared by all consumer warps and joined by the
+//                bounded barrier comb[s]), each warp arrives on cdone[s];
+//   finisher  -- waits cdone[s], takes the item's sums, frees the stage
+//                (empty[s]), then does the device-scope bookkeeping: the
+//                tile count, the alpha/beta finalisation of the last L tile
+//                and the progress release.
+// No CTA-wide barrier is used after set-up, so warps that finish a tile
+// early move on to the next one.
 template <int N1L, int NHL, int N1R, int NHR, int CW>
 __global__ void __maxnreg__(PRegs<CW>::value)
     k_lanczos_persistent(const __grid_constant__ CUtensorMap vmap, PersistentLanczos p) {
-  constexpr int kConsumerWarps = CW;
   constexpr int kConsumers = CW * 32;
   using PS = PShape<N1L, NHL, N1R, NHR>;
   using PR = typename PS::PR;
   using PL = typename PS::PL;
   constexpr int HL = PS::HL, HR = PS::HR, TR = PS::TR, RS = PR::RS;
   constexpr long long QUARTER = (long long)HL * HR;
+  constexpr int OREC_R = ((PR::NO * 24) + 15) / 16 * 16;
+  constexpr int OREC_L = ((PL::NO * 24) + 15) / 16 * 16;
+  static_assert(OREC_R <= PS::OREC_BYTES && OREC_L <= PS::OREC_BYTES, "outer records exceed their stage slot");
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-  __shared__ __align__(8) unsigned long long full_bar[2], empty_bar[2];
+  __shared__ __align__(8) unsigned long long full_bar[2], empty_bar[2], cdone_bar[2], comb_bar[2];
   __shared__ Item meta[2];
-  __shared__ double red[kConsumerWarps][3];
-  __shared__ const float2* tab_ptr[2][kTabCache];  // per vector: pass-R / pass-L coefficient tables
+  __shared__ double red[2][CW][3];
+  __shared__ const void* tab_ptr[4][kTabCache];  // per vector: tabR, tabL, orecR, orecL
   auto stage_tab = [&](int s) { return reinterpret_cast<float2*>(base + s * PS::STAGE); };
   auto stage_orec = [&](int s) { return reinterpret_cast<ORec<float2>*>(base + s * PS::STAGE + PS::TAB_BYTES); };
   auto stage_tile = [&](int s) {
     return reinterpret_cast<float2*>(base + s * PS::STAGE + PS::TAB_BYTES + PS::OREC_BYTES);
   };
+  auto view_ptrs = [&](int b, const void*(&out)[4]) {
+    if (b < kTabCache) {
+      for (int k = 0; k < 4; ++k) out[k] = tab_ptr[k][b];
+    } else {
+      const CubeView<float2>* v = p.views + (p.sys_of ? p.sys_of[b] : 0);
+      out[0] = v->tabR;
+      out[1] = v->tabL;
+      out[2] = v->orecR;
+      out[3] = v->orecL;
+    }
+  };
   if (threadIdx.x == 0) {
     for (int s = 0; s < 2; ++s) {
       mbar_init(&full_bar[s], 1);
       mbar_init(&empty_bar[s], 1);
+      mbar_init(&cdone_bar[s], CW);
+      mbar_init(&comb_bar[s], CW);
     }
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
@@ -258,13 +273,15 @@ __global__ void __maxnreg__(PRegs<CW>::value)
     const CubeView<float2>* v = p.views + (p.sys_of ? p.sys_of[b] : 0);
     tab_ptr[0][b] = v->tabR;
     tab_ptr[1][b] = v->tabL;
+    tab_ptr[2][b] = v->orecR;
+    tab_ptr[3][b] = v->orecL;
   }
   __syncthreads();
   const int mseg = p.j1 - p.j0;
   const long long total = (long long)mseg * p.nb * PS::PT;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-  if (warp == kConsumerWarps) {
+  if (warp == CW) {
     // ----------------------------- producer -----------------------------
     // per stage: the last use armed (copies or end) and whether it got copies
     long long armed_use[2] = {-1, -1};
@@ -309,29 +326,22 @@ __global__ void __maxnreg__(PRegs<CW>::value)
       // stage the item's data (also for a vector that stopped: the consumers
       // read its skip flag and leave the staged data unused)
       fence_proxy_async();
-      const float2* tabR;
-      const float2* tabL;
-      if (m.b < kTabCache) {
-        tabR = tab_ptr[0][m.b];
-        tabL = tab_ptr[1][m.b];
-      } else {
-        const CubeView<float2>* view = p.views + (p.sys_of ? p.sys_of[m.b] : 0);
-        tabR = view->tabR;
-        tabL = view->tabL;
-      }
+      const void* ptrs[4];
+      view_ptrs(m.b, ptrs);
       const float2* vj = p.V + (long long)m.b * p.vstride + (long long)m.j * p.ld;
       float2* tile = stage_tile(s);
       if (m.kind == 0) {
         const int row0 = m.tile * TR;
         const int rows = min(TR, 2 * HL - row0);
         const bool prev = m.j > 0;
-        const unsigned bytes = (unsigned)(rows * 2 * HR * 8 * (prev ? 2 : 1) + PS::SR::NTAB * 8);
+        const unsigned bytes = (unsigned)(rows * 2 * HR * 8 * (prev ? 2 : 1) + PS::SR::NTAB * 8 + OREC_R);
         if (lane == 0) {
           meta[s] = m;
           mbar_arrive_expect_tx(&full_bar[s], bytes);
         }
         __syncwarp();
-        if (lane == 0) bulk_g2s(stage_tab(s), tabR, PS::SR::NTAB * 8, &full_bar[s]);
+        if (lane == 0) bulk_g2s(stage_tab(s), ptrs[0], PS::SR::NTAB * 8, &full_bar[s]);
+        if (lane == 1) bulk_g2s(stage_orec(s), ptrs[2], OREC_R, &full_bar[s]);
         const int rr = lane & 15, which = lane >> 4;
         if (rr < rows && (which == 0 || prev)) {
           const float2* src = which == 0 ? vj : vj - p.ld;
@@ -343,15 +353,17 @@ __global__ void __maxnreg__(PRegs<CW>::value)
           bulk_g2s(dst + HR, src + g + QUARTER, HR * 8, &full_bar[s]);
         }
       } else {
-        const unsigned bytes = (unsigned)(PS::L_TILE_BYTES + PS::SL::NTAB * 8);
+        const unsigned bytes = (unsigned)(PS::L_TILE_BYTES + PS::SL::NTAB * 8 + OREC_L);
         if (lane == 0) {
           meta[s] = m;
           mbar_arrive_expect_tx(&full_bar[s], bytes);
         }
         __syncwarp();
-        if (lane == 0) bulk_g2s(stage_tab(s), tabL, PS::SL::NTAB * 8, &full_bar[s]);
-        if (lane < 2 * PS::LSPLIT) {
-          const int ea = lane / PS::LSPLIT, part = lane % PS::LSPLIT;
+        if (lane == 0) bulk_g2s(stage_tab(s), ptrs[1], PS::SL::NTAB * 8, &full_bar[s]);
+        if (lane == 1) bulk_g2s(stage_orec(s), ptrs[3], OREC_L, &full_bar[s]);
+        if (lane >= 2 && lane < 2 + 2 * PS::LSPLIT) {
+          const int q = lane - 2;
+          const int ea = q / PS::LSPLIT, part = q % PS::LSPLIT;
           const long long slot = p.slot0 + (long long)m.b * (p.m + 1) + m.j;
           tma_5d(tile + (ea * HL + part * PS::BL) * 16, &vmap, m.tile * 8, 0, part * PS::BL, ea, (int)slot,
                  &full_bar[s]);
@@ -368,28 +380,99 @@ __global__ void __maxnreg__(PRegs<CW>::value)
     return;
   }
 
+  if (warp == CW + 1) {
+    // ----------------------------- finisher -----------------------------
+    for (long long it = 0;; ++it) {
+      const int s = (int)(it & 1);
+      bool ok = true;
+      if (lane == 0) ok = mbar_wait(&cdone_bar[s], (unsigned)((it >> 1) & 1), p.status);
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) break;
+      const Item m = meta[s];
+      if (m.kind < 0) break;
+      if (lane == 0) {
+        const int b = m.b;
+        const bool skip = *reinterpret_cast<volatile int*>(p.skip + (long long)b * p.istride) != 0;
+        double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+        if (m.kind == 1 && !skip)
+          for (int w = 0; w < CW; ++w) {
+            t0 += red[s][w][0];
+            t1 += red[s][w][1];
+            t2 += red[s][w][2];
+          }
+        mbar_arrive(&empty_bar[s]);  // the stage's data and sums are no longer needed
+        // the consumers' global writes (ordered before this thread by cdone)
+        // become visible device-wide before the tile is counted
+        __threadfence();
+        fence_proxy_async();
+        if (m.kind == 1 && !skip) {
+          double* part = p.part + (long long)b * p.part_stride + m.tile * 3;
+          part[0] = t0;
+          part[1] = t1;
+          part[2] = t2;
+          __threadfence();
+        }
+        const int ntiles = m.kind == 0 ? PS::RT : PS::LT;
+        const unsigned done = atomicAdd(p.cnt + b, 1u);
+        if (done == (unsigned)ntiles - 1) {
+          __threadfence();
+          p.cnt[b] = 0;
+          if (m.kind == 1 && !skip) {
+            // alpha_j, beta_j and the breakdown test from the tiles' sums, in tile order
+            double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+            const double* pt = p.part + (long long)b * p.part_stride;
+            for (int k = 0; k < PS::LT; ++k) {
+              s0 += __ldcg(pt + 3 * k);
+              s1 += __ldcg(pt + 3 * k + 1);
+              s2 += __ldcg(pt + 3 * k + 2);
+            }
+            const double alpha = s2 > 0.0 ? s0 / s2 : 0.0;
+            p.alpha[(long long)b * p.dstride + m.j] = alpha;
+            if (m.j < p.m - 1) {
+              const double beta = sqrt(fmax(s1 - s0 * alpha, 0.0));  // |w' - alpha v_j|
+              p.beta[(long long)b * p.dstride + m.j] = beta;
+              p.scale[(long long)b * p.dstride] = beta > 0.0 ? 1.0 / beta : 0.0;
+              const double ref = fabs(alpha) + (m.j == 0 ? 0.0 : p.beta[(long long)b * p.dstride + m.j - 1]);
+              if (!(beta > p.breakdown_rel * ref)) {
+                p.stop[(long long)b * p.istride] = 1;
+                p.skip[(long long)b * p.istride] = 1;
+                p.msize[(long long)b * p.istride] = m.j + 1;
+              }
+            }
+            __threadfence();
+          }
+          st_release(p.prog + b, m.kind == 0 ? 2 * m.j + 1 : 2 * m.j + 2);
+        }
+      }
+      __syncwarp();
+    }
+    return;
+  }
+
   // ----------------------------- consumers -----------------------------
   const int tid = threadIdx.x;  // 0 .. kConsumers - 1
+  unsigned comb_use[2] = {0u, 0u};
   for (long long it = 0;; ++it) {
     const int s = (int)(it & 1);
-    const unsigned parity = (unsigned)((it >> 1) & 1);
-    const bool ok = consumers_and<kConsumers>(mbar_wait(&full_bar[s], parity, p.status));
-    if (!ok) break;
-    Item m = meta[s];
-    if (m.kind < 0) break;
+    if (!mbar_wait(&full_bar[s], (unsigned)((it >> 1) & 1), p.status)) break;
+    const Item m = meta[s];
+    if (m.kind < 0) {
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&cdone_bar[s]);  // lets the finisher see the end
+      break;
+    }
     // a vector stopped by a breakdown (or finished before this Krylov step)
     // keeps its counters moving but does no arithmetic; the flag was set
     // before the progress this item waited for
-    m.skip = *reinterpret_cast<volatile int*>(p.skip + (long long)m.b * p.istride);
-    float2* tab = stage_tab(s);
-    ORec<float2>* orec = stage_orec(s);
-    float2* tile = stage_tile(s);
-    const int b = m.b;
-    const CubeView<float2>* view = p.views + (p.sys_of ? p.sys_of[b] : 0);
-    float2* vj = p.V + (long long)b * p.vstride + (long long)m.j * p.ld;
-    float2* yb = p.ya + (long long)b * p.ld;
-    double dot = 0.0, nw = 0.0, nv = 0.0;
-    if (!m.skip) {
+    const bool skip = *reinterpret_cast<volatile int*>(p.skip + (long long)m.b * p.istride) != 0;
+    bool ok = true;
+    if (!skip) {
+      float2* tab = stage_tab(s);
+      const ORec<float2>* orec = stage_orec(s);
+      float2* tile = stage_tile(s);
+      const int b = m.b;
+      float2* vj = p.V + (long long)b * p.vstride + (long long)m.j * p.ld;
+      float2* yb = p.ya + (long long)b * p.ld;
       if (m.kind == 0) {
         const int row0 = m.tile * TR;
         const int rows = min(TR, 2 * HL - row0);
@@ -419,80 +502,33 @@ __global__ void __maxnreg__(PRegs<CW>::value)
             *reinterpret_cast<float4*>(tile + slot) = v;
             *reinterpret_cast<float4*>(vj + g) = v;
           }
+          // every consumer warp's share is combined before any warp reads the rows
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&comb_bar[s]);
+          ok = mbar_wait(&comb_bar[s], comb_use[s] & 1u, p.status);
+          ++comb_use[s];
         }
-        build_orec<float2, typename PS::SR, PS::SR::K - 2, 4>(tab, orec, PR::NO, tid, kConsumers);
-        consumers_sync<kConsumers>();
-        r_tile_math<float2, N1R, NHR>(tab, orec, tile, ptile, rows, row0, HL, QUARTER, yb, 1.0f, bprev, prev, warp,
-                                      kConsumerWarps);
+        if (ok)
+          r_tile_math<float2, N1R, NHR>(tab, orec, tile, ptile, rows, row0, HL, QUARTER, yb, 1.0f, bprev, prev, warp,
+                                        CW);
       } else {
-        build_orec<float2, typename PS::SL, PS::SL::K - 3, 8>(tab, orec, PL::NO, tid, kConsumers);
-        consumers_sync<kConsumers>();
+        const CubeView<float2>* view = p.views + (p.sys_of ? p.sys_of[b] : 0);
+        double dot = 0.0, nw = 0.0, nv = 0.0;
         l_tile_math<float2, N1L, NHL>(tab, orec, tile, view, m.tile * 8, QUARTER, yb, vj + p.ld, 1.0f,
-                                      m.j < p.m - 1, warp, kConsumerWarps, dot, nw, nv);
+                                      m.j < p.m - 1, warp, CW, dot, nw, nv);
         dot = warp_sum_d(dot);
         nw = warp_sum_d(nw);
         nv = warp_sum_d(nv);
         if (lane == 0) {
-          red[warp][0] = dot;
-          red[warp][1] = nw;
-          red[warp][2] = nv;
+          red[s][warp][0] = dot;
+          red[s][warp][1] = nw;
+          red[s][warp][2] = nv;
         }
       }
     }
-    // the CTA barrier orders every consumer's global writes before thread 0's
-    // device-scope fence and counter update (the grid-barrier pattern);
-    // readers on other SMs acquire the progress counter, and their producer
-    // fences the async proxy before its tensor copies
-    consumers_sync<kConsumers>();
-    if (tid == 0) {
-      __threadfence();
-      fence_proxy_async();
-      const int ntiles = m.kind == 0 ? PS::RT : PS::LT;
-      if (m.kind == 1 && !m.skip) {
-        double t0 = 0.0, t1 = 0.0, t2 = 0.0;
-        for (int w = 0; w < kConsumerWarps; ++w) {
-          t0 += red[w][0];
-          t1 += red[w][1];
-          t2 += red[w][2];
-        }
-        double* part = p.part + (long long)b * p.part_stride + m.tile * 3;
-        part[0] = t0;
-        part[1] = t1;
-        part[2] = t2;
-        __threadfence();
-      }
-      const unsigned done = atomicAdd(p.cnt + b, 1u);
-      if (done == (unsigned)ntiles - 1) {
-        __threadfence();
-        p.cnt[b] = 0;
-        if (m.kind == 1 && !m.skip) {
-          // alpha_j, beta_j and the breakdown test from the tiles' sums, in tile order
-          double t0 = 0.0, t1 = 0.0, t2 = 0.0;
-          const double* part = p.part + (long long)b * p.part_stride;
-          for (int k = 0; k < PS::LT; ++k) {
-            t0 += __ldcg(part + 3 * k);
-            t1 += __ldcg(part + 3 * k + 1);
-            t2 += __ldcg(part + 3 * k + 2);
-          }
-          const double alpha = t2 > 0.0 ? t0 / t2 : 0.0;
-          p.alpha[(long long)b * p.dstride + m.j] = alpha;
-          if (m.j < p.m - 1) {
-            const double beta = sqrt(fmax(t1 - t0 * alpha, 0.0));  // |w' - alpha v_j|
-            p.beta[(long long)b * p.dstride + m.j] = beta;
-            p.scale[(long long)b * p.dstride] = beta > 0.0 ? 1.0 / beta : 0.0;
-            const double ref = fabs(alpha) + (m.j == 0 ? 0.0 : p.beta[(long long)b * p.dstride + m.j - 1]);
-            if (!(beta > p.breakdown_rel * ref)) {
-              p.stop[(long long)b * p.istride] = 1;
-              p.skip[(long long)b * p.istride] = 1;
-              p.msize[(long long)b * p.istride] = m.j + 1;
-            }
-          }
-          __threadfence();
-        }
-        st_release(p.prog + b, m.kind == 0 ? 2 * m.j + 1 : 2 * m.j + 2);
-      }
-      mbar_arrive(&empty_bar[s]);
-    }
+    if (!ok) break;
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&cdone_bar[s]);
   }
 }
 
@@ -539,7 +575,7 @@ template <int N1L, int NHL, int N1R, int NHR, int CW>
 void launch_instance(const PersistentLanczos& p, const float2* V_base, long long nslots, cudaStream_t st) {
   using PS = PShape<N1L, NHL, N1R, NHR>;
   static_assert(PS::SMEM <= 227 * 1024, "persistent Lanczos stages exceed shared memory");
-  constexpr int kThreads = CW * 32 + 32;
+  constexpr int kThreads = CW * 32 + 64;
   auto kern = k_lanczos_persistent<N1L, NHL, N1R, NHR, CW>;
   {
     static std::mutex mu;
@@ -565,17 +601,17 @@ void launch_instance(const PersistentLanczos& p, const float2* V_base, long long
 
 using Launcher = void (*)(const PersistentLanczos&, const float2*, long long, cudaStream_t);
 
-// Consumer warps per CTA (8, 11 or 12; set by rpm_set_persistent_warps):
-// 8 and 11 keep 168 registers per thread, 12 (two pass-R and three pass-L
-// warp tasks per warp on the full system) caps them at 128.
-std::atomic<int> g_consumer_warps{11};
+// Consumer warps per CTA (8 or 10; set by rpm_set_persistent_warps): with the
+// producer and finisher warps both keep 168 registers per thread; 8 splits
+// the full system's 24 pass-R warp tasks evenly (the combine barrier waits
+// for the slowest warp), 10 hides more latency.
+std::atomic<int> g_consumer_warps{8};
 
 template <int N1L, int NHL, int N1R, int NHR>
 Launcher by_warps(int warps) {
   switch (warps) {
-    case 8: return launch_instance<N1L, NHL, N1R, NHR, 8>;
-    case 12: return launch_instance<N1L, NHL, N1R, NHR, 12>;
-    default: return launch_instance<N1L, NHL, N1R, NHR, 11>;
+    case 10: return launch_instance<N1L, NHL, N1R, NHR, 10>;
+    default: return launch_instance<N1L, NHL, N1R, NHR, 8>;
   }
 }
 
@@ -619,8 +655,7 @@ bool launch_lanczos_persistent(const PersistentLanczos& p, const CubePlan& plan,
 
 extern "C" int rpm_set_persistent_warps(int consumer_warps) {
   return rpm::guarded([&] {
-    if (consumer_warps != 8 && consumer_warps != 11 && consumer_warps != 12)
-      rpm::fail(RPM_E_INVALID, "consumer warps must be 8, 11 or 12");
+    if (consumer_warps != 8 && consumer_warps != 10) rpm::fail(RPM_E_INVALID, "consumer warps must be 8 or 10");
     rpm::g_consumer_warps.store(consumer_warps, std::memory_order_relaxed);
   });
 }

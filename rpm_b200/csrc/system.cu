@@ -193,6 +193,37 @@ static T* upload(rpm_system* sys, const void* src, size_t bytes) {
   return static_cast<T*>(p);
 }
 
+// Outer-index records of the shape-specialised passes (see CubeView): for
+// outer index o the electron-only diagonal / flip entries plus those of the
+// outer digits k < nout, digit value (o / (gs[k] / div)) % dim[k], summed in
+// FP32 in digit order (the order the passes' own record builder uses).
+static std::vector<float> outer_records(const CubeSide& side, const std::vector<float2>& tab, int nout, int div) {
+  const int no = side.half / div;
+  std::vector<float> out((size_t)no * 6 + 2, 0.0f);  // + padding to 16 bytes when no is odd
+  for (int o = 0; o < no; ++o) {
+    float d[2] = {tab[0].x, tab[1].x};
+    float2 f[2] = {tab[2], tab[3]};
+    for (int k = 0; k < nout; ++k) {
+      const int m = (o / (side.gs[k] / div)) % side.dim[k];
+      for (int e = 0; e < 2; ++e) {
+        d[e] += tab[side.offD[k] + e * side.dim[k] + m].x;
+        const float2 g = tab[side.offF[k] + e * side.dim[k] + m];
+        f[e].x += g.x;
+        f[e].y += g.y;
+      }
+    }
+    float* r = out.data() + (size_t)o * 6;
+    r[0] = d[0];
+    r[1] = d[1];
+    r[2] = f[0].x;
+    r[3] = f[0].y;
+    r[4] = f[1].x;
+    r[5] = f[1].y;
+  }
+  out.resize(((size_t)no * 24 + 15) / 16 * 4);
+  return out;
+}
+
 static std::vector<double2> to_d2(const std::vector<cd>& v) {
   std::vector<double2> out(v.size());
   for (size_t i = 0; i < v.size(); ++i) out[i] = make_double2(v[i].real(), v[i].imag());
@@ -270,6 +301,18 @@ static void upload_system(rpm_system* sys) {
       c64.nr = c32.nr = sys->nr;
       c64.half_l = c32.half_l = sys->half_l;
       c64.half_r = c32.half_r = sys->half_r;
+      c64.orecR = c64.orecL = c32.orecR = c32.orecL = nullptr;
+      c64.orec_bytes_r = c64.orec_bytes_l = c32.orec_bytes_r = c32.orec_bytes_l = 0;
+      const CubeSide& cl = sys->cube_l;
+      const CubeSide& cr = sys->cube_r;
+      if (c32.inner_r >= 2 && c32.inner_l >= 3 && cr.half % 4 == 0 && cl.half % 8 == 0) {
+        const std::vector<float> rr = outer_records(cr, tr32, cr.K - 2, 4);
+        const std::vector<float> rl = outer_records(cl, tl32, cl.K - 3, 8);
+        c32.orecR = upload<float>(sys, rr.data(), rr.size() * sizeof(float));
+        c32.orecL = upload<float>(sys, rl.data(), rl.size() * sizeof(float));
+        c32.orec_bytes_r = (int)(rr.size() * sizeof(float));
+        c32.orec_bytes_l = (int)(rl.size() * sizeof(float));
+      }
       sys->cube64_dev = upload<CubeView<double2>>(sys, &c64, sizeof(c64));
       sys->cube32_dev = upload<CubeView<float2>>(sys, &c32, sizeof(c32));
     }

@@ -34,7 +34,7 @@ def _plain_yield(rb, h, psi, times, dims):
     return ref.observable_values, rb.integrate_yield(times, ref.observable_values, 1.0)
 
 
-@pytest.mark.parametrize("warps", [11, 8, 12])
+@pytest.mark.parametrize("warps", [8, 10])
 @pytest.mark.parametrize("which,nvec,wavefront,krylov", [("prefix", 7, 3, 16), ("full", 6, 12, 16),
                                                          ("full", 5, 2, 24)])
 def test_persistent_matches_pass_launches(which, nvec, wavefront, krylov, warps):
@@ -54,7 +54,7 @@ def test_persistent_matches_pass_launches(which, nvec, wavefront, krylov, warps)
         out[kind] = bp.propagate(list(states), times, system_index=index, lifetime_us=1.0)
         assert bp.lanczos_kind() == kind
         assert not np.any(out[kind].status)
-    _lib.call("rpm_set_persistent_warps", 11)
+    _lib.call("rpm_set_persistent_warps", 8)
     a, b = out["persistent"], out["passes"]
     assert np.max(np.abs(a.observable_values - b.observable_values)) < SAME_TOL
     assert np.max(np.abs(a.yields - b.yields)) < SAME_TOL

@@ -101,6 +101,10 @@ def test_stage_layout_and_copy_addresses(shape):
     for nt in (ps.NTAB_R, ps.NTAB_L):
         assert nt * 8 % 16 == 0 and nt * 8 <= ps.TAB_BYTES
     assert max(ps.HR // 4, ps.HL // 8) * ORREC <= ps.OREC_BYTES
+    # outer-index records: one bulk copy each, padded to 16 bytes, inside the slot
+    for no in (ps.HR // 4, ps.HL // 8):
+        padded = (no * ORREC + 15) // 16 * 16
+        assert padded % 16 == 0 and padded <= ps.OREC_BYTES
     ld = (ps.N + 63) // 64 * 64
     m = 40
     vstride = (m + 1) * ld
