@@ -120,6 +120,14 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
 __device__ __forceinline__ void st_release(int* p, int v) {
   asm volatile("st.release.gpu.global.b32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
 }
+// Device-scope acquire-release fetch-and-add: earlier writes this thread
+// performed or observed become visible before the update, and later reads see
+// what the other updaters published before theirs.
+__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;\n" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
 // Wait until *p >= need (acquire); false after the time limit or a raised status.
 __device__ bool wait_progress(const int* p, int need, int* status) {
   const long long t0 = clock64();
@@ -213,18 +221,21 @@ struct PRegs {
   static constexpr int value = raw > 255 ? 255 : raw;
 };
 
-// Per stage (two stages), the item moves through three roles:
+// An item moves through three roles:
 //   producer  -- dequeues, waits for the item's dependency, stages tiles,
-//                table and outer records by TMA, completes full[s];
+//                table and outer records by TMA into stage s (two stages),
+//                completes full[s];
 //   consumers -- wait full[s], compute their warp tasks (the pass-R combine
 //                of v_j is shared by all consumer warps and joined by the
-//                bounded barrier comb[s]), each warp arrives on cdone[s];
-//   finisher  -- waits cdone[s], takes the item's sums, frees the stage
-//                (empty[s]), then does the device-scope bookkeeping: the
-//                tile count, the alpha/beta finalisation of the last L tile
-//                and the progress release.
-// No CTA-wide barrier is used after set-up, so warps that finish a tile
-// early move on to the next one.
+//                bounded barrier comb[s]), leave the item record and their
+//                L sums in slot q of a ring (kRing slots) and arrive on
+//                empty[s] and cdone[q];
+//   finisher  -- waits cdone[q], takes the record, frees the slot (ffree[q])
+//                and does the device-scope bookkeeping: the tile count, the
+//                alpha/beta finalisation of the last L tile and the progress
+//                release.
+// No CTA-wide barrier is used after set-up, warps that finish a tile early
+// move on to the next one, and the finisher may lag kRing items behind.
 template <int N1L, int NHL, int N1R, int NHR, int CW>
 __global__ void __maxnreg__(PRegs<CW>::value)
     k_lanczos_persistent(const __grid_constant__ CUtensorMap vmap, PersistentLanczos p) {
@@ -240,9 +251,12 @@ __global__ void __maxnreg__(PRegs<CW>::value)
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-  __shared__ __align__(8) unsigned long long full_bar[2], empty_bar[2], cdone_bar[2], comb_bar[2];
+  constexpr int kRing = 4;
+  __shared__ __align__(8) unsigned long long full_bar[2], empty_bar[2], comb_bar[2], cdone_bar[kRing],
+      ffree_bar[kRing];
   __shared__ Item meta[2];
-  __shared__ double red[2][CW][3];
+  __shared__ Item fmeta[kRing];
+  __shared__ double red[kRing][CW][3];
   __shared__ const void* tab_ptr[4][kTabCache];  // per vector: tabR, tabL, orecR, orecL
   auto stage_tab = [&](int s) { return reinterpret_cast<float2*>(base + s * PS::STAGE); };
   auto stage_orec = [&](int s) { return reinterpret_cast<ORec<float2>*>(base + s * PS::STAGE + PS::TAB_BYTES); };
@@ -263,9 +277,12 @@ __global__ void __maxnreg__(PRegs<CW>::value)
   if (threadIdx.x == 0) {
     for (int s = 0; s < 2; ++s) {
       mbar_init(&full_bar[s], 1);
-      mbar_init(&empty_bar[s], 1);
-      mbar_init(&cdone_bar[s], CW);
+      mbar_init(&empty_bar[s], CW);
       mbar_init(&comb_bar[s], CW);
+    }
+    for (int q = 0; q < kRing; ++q) {
+      mbar_init(&cdone_bar[q], CW);
+      mbar_init(&ffree_bar[q], 1);
     }
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
@@ -383,41 +400,38 @@ __global__ void __maxnreg__(PRegs<CW>::value)
   if (warp == CW + 1) {
     // ----------------------------- finisher -----------------------------
     for (long long it = 0;; ++it) {
-      const int s = (int)(it & 1);
+      const int q = (int)(it % kRing);
       bool ok = true;
-      if (lane == 0) ok = mbar_wait(&cdone_bar[s], (unsigned)((it >> 1) & 1), p.status);
+      if (lane == 0) ok = mbar_wait(&cdone_bar[q], (unsigned)((it / kRing) & 1), p.status);
       ok = __shfl_sync(0xffffffffu, ok, 0);
       if (!ok) break;
-      const Item m = meta[s];
+      const Item m = fmeta[q];
       if (m.kind < 0) break;
       if (lane == 0) {
         const int b = m.b;
-        const bool skip = *reinterpret_cast<volatile int*>(p.skip + (long long)b * p.istride) != 0;
         double t0 = 0.0, t1 = 0.0, t2 = 0.0;
-        if (m.kind == 1 && !skip)
+        if (m.kind == 1 && !m.skip)
           for (int w = 0; w < CW; ++w) {
-            t0 += red[s][w][0];
-            t1 += red[s][w][1];
-            t2 += red[s][w][2];
+            t0 += red[q][w][0];
+            t1 += red[q][w][1];
+            t2 += red[q][w][2];
           }
-        mbar_arrive(&empty_bar[s]);  // the stage's data and sums are no longer needed
-        // the consumers' global writes (ordered before this thread by cdone)
-        // become visible device-wide before the tile is counted
-        __threadfence();
-        fence_proxy_async();
-        if (m.kind == 1 && !skip) {
+        mbar_arrive(&ffree_bar[q]);  // the slot's record and sums are taken
+        if (m.kind == 1 && !m.skip) {
           double* part = p.part + (long long)b * p.part_stride + m.tile * 3;
           part[0] = t0;
           part[1] = t1;
           part[2] = t2;
-          __threadfence();
         }
+        // the consumers' global writes (ordered before this thread by cdone)
+        // and the sums become visible device-wide with the count; the last
+        // tile of a phase sees every other tile's sums
+        fence_proxy_async();
         const int ntiles = m.kind == 0 ? PS::RT : PS::LT;
-        const unsigned done = atomicAdd(p.cnt + b, 1u);
+        const unsigned done = atom_add_acq_rel(p.cnt + b, 1u);
         if (done == (unsigned)ntiles - 1) {
-          __threadfence();
           p.cnt[b] = 0;
-          if (m.kind == 1 && !skip) {
+          if (m.kind == 1 && !m.skip) {
             // alpha_j, beta_j and the breakdown test from the tiles' sums, in tile order
             double s0 = 0.0, s1 = 0.0, s2 = 0.0;
             const double* pt = p.part + (long long)b * p.part_stride;
@@ -439,7 +453,6 @@ __global__ void __maxnreg__(PRegs<CW>::value)
                 p.msize[(long long)b * p.istride] = m.j + 1;
               }
             }
-            __threadfence();
           }
           st_release(p.prog + b, m.kind == 0 ? 2 * m.j + 1 : 2 * m.j + 2);
         }
@@ -455,16 +468,21 @@ __global__ void __maxnreg__(PRegs<CW>::value)
   for (long long it = 0;; ++it) {
     const int s = (int)(it & 1);
     if (!mbar_wait(&full_bar[s], (unsigned)((it >> 1) & 1), p.status)) break;
-    const Item m = meta[s];
+    Item m = meta[s];
+    const int q = (int)(it % kRing);
+    // the ring slot of this item is free once the finisher took item it - kRing
+    if (it >= kRing && !mbar_wait(&ffree_bar[q], (unsigned)((it / kRing - 1) & 1), p.status)) break;
     if (m.kind < 0) {
+      if (warp == 0 && lane == 0) fmeta[q] = m;
       __syncwarp();
-      if (lane == 0) mbar_arrive(&cdone_bar[s]);  // lets the finisher see the end
+      if (lane == 0) mbar_arrive(&cdone_bar[q]);  // lets the finisher see the end
       break;
     }
     // a vector stopped by a breakdown (or finished before this Krylov step)
     // keeps its counters moving but does no arithmetic; the flag was set
     // before the progress this item waited for
     const bool skip = *reinterpret_cast<volatile int*>(p.skip + (long long)m.b * p.istride) != 0;
+    m.skip = skip ? 1 : 0;
     bool ok = true;
     if (!skip) {
       float2* tab = stage_tab(s);
@@ -520,15 +538,19 @@ __global__ void __maxnreg__(PRegs<CW>::value)
         nw = warp_sum_d(nw);
         nv = warp_sum_d(nv);
         if (lane == 0) {
-          red[s][warp][0] = dot;
-          red[s][warp][1] = nw;
-          red[s][warp][2] = nv;
+          red[q][warp][0] = dot;
+          red[q][warp][1] = nw;
+          red[q][warp][2] = nv;
         }
       }
     }
     if (!ok) break;
+    if (warp == 0 && lane == 0) fmeta[q] = m;
     __syncwarp();
-    if (lane == 0) mbar_arrive(&cdone_bar[s]);
+    if (lane == 0) {
+      mbar_arrive(&empty_bar[s]);  // this warp no longer reads the stage
+      mbar_arrive(&cdone_bar[q]);
+    }
   }
 }
 
