@@ -304,7 +304,7 @@ class CompiledFullPairHamiltonian:
         psi = grouped.reshape(self.left_dimension, self.right_dimension)
         out = self.left_operator @ psi + (self.right_operator @ psi.T).T
         four = grouped.reshape(2, self.left_dimension // 2, 2, self.right_dimension // 2)
-        out += np.einsum("abcd,cxdy->axby", self.electron_pair_operator, four).reshape(psi.shape)
+        out += np.einsum("abcd,cxdy->axby", self.electron_pair_operator, four, optimize=True).reshape(psi.shape)
         back = np.transpose(out.reshape(self.left_dimensions + self.right_dimensions), self.inverse_permutation)
         self.matvec_count += 1
         return back.reshape(-1)
@@ -502,19 +502,23 @@ class AdaptiveLanczosPropagator:
             raise ValueError("Cannot propagate the zero vector.")
         m = min(int(target), state.size)
         v = np.empty((state.size, m), dtype=complex)
+        # rows of vh are the conjugated basis vectors, kept up to date so the
+        # projections need no conjugate copy of the block
+        vh = np.empty((m, state.size), dtype=complex)
         alpha = np.empty(m)
         beta = np.empty(max(m - 1, 0))
         v[:, 0] = state / norm
+        np.conjugate(v[:, 0], out=vh[0])
         size = m
         for j in range(m):
             w = self.hamiltonian.matvec(v[:, j])
             alpha[j] = float(np.vdot(v[:, j], w).real)
-            w = w - alpha[j] * v[:, j]
+            w -= alpha[j] * v[:, j]
             if j:
-                w = w - beta[j - 1] * v[:, j - 1]
-            block = v[:, : j + 1]
+                w -= beta[j - 1] * v[:, j - 1]
+            block, block_h = v[:, : j + 1], vh[: j + 1]
             for _ in range(2):
-                w = w - block @ (block.conj().T @ w)
+                w -= block @ (block_h @ w)
             if j == m - 1:
                 break
             b = float(np.linalg.norm(w))
@@ -523,6 +527,7 @@ class AdaptiveLanczosPropagator:
                 size = j + 1
                 break
             v[:, j + 1] = w / b
+            np.conjugate(v[:, j + 1], out=vh[j + 1])
         return v[:, :size], alpha[:size], beta[: max(0, size - 1)]
 
     def _candidate(self, alpha, beta, dimension, time_us, state_norm):
