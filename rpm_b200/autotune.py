@@ -26,8 +26,8 @@ meets the same local tolerance as in the full run (the Hamiltonian is time
 independent, so the cost per simulated microsecond is stationary), and is
 scored in trajectory-microseconds per second.  A candidate is eligible only if
 its prefix yields agree with a tight-budget run of the same trajectories
-within ``accuracy * prefix / horizon`` (errors accumulate over the horizon):
-speed never buys accuracy.  Trial trajectories are drawn round-robin over the
+within ``accuracy`` (half the yield tolerance by default): speed never buys
+accuracy.  Trial trajectories are drawn round-robin over the
 sample's shapes (system dimensions), so uneven batches are represented.
 """
 
@@ -138,8 +138,8 @@ def tune(hamiltonians: Sequence, states, system_index: Sequence[int], *, horizon
     candidate propagates ``tile`` of them, spread over the sample's shapes,
     over ``horizon_us`` with the budget scaled to that prefix; it is eligible
     when its prefix yields are within ``accuracy`` (default: half the yield
-    tolerance) x prefix / horizon of a run at a hundredth of the budget with
-    the largest Krylov dimension.  Tiles whose Krylov basis would need more
+    tolerance) of a run at a hundredth of the budget with the largest Krylov
+    dimension.  Tiles whose Krylov basis would need more
     than ``memory_fraction`` of the free device memory are skipped.  With
     ``cache`` the result is stored in (and reused from) that JSON file, keyed
     by the systems' dimensions, the device name and the search space.
@@ -165,7 +165,7 @@ def tune(hamiltonians: Sequence, states, system_index: Sequence[int], *, horizon
     times = np.arange(int(round(horizon_us / grid_us)) + 1) * grid_us
     frac = horizon_us / full_horizon_us
     trial_budget = budget * frac
-    gate = accuracy * frac
+    gate = accuracy
     ld = max(h.dimension for h in hams)
     shapes = [(tuple(h.dimensions), tuple(getattr(h, "left_axes", ()))) for h in hams]
     # tight-budget reference yields of every trajectory any tile uses
@@ -190,8 +190,7 @@ def tune(hamiltonians: Sequence, states, system_index: Sequence[int], *, horizon
                 rate = tile * horizon_us / secs
                 err = float(np.max(np.abs(ys - np.array([ref_of[int(p)] for p in sel])))) if ys is not None else None
                 ok = err is not None and err <= gate
-                trials.append({**trial, "seconds": secs, "throughput": rate, "yield_err_prefix": err,
-                               "yield_err_per_horizon": None if err is None else err / frac, "accepted": ok})
+                trials.append({**trial, "seconds": secs, "throughput": rate, "yield_err_prefix": err, "accepted": ok})
                 if ok and (best is None or rate > best[0]):
                     best = (rate, m, tile, reorth)
     if best is None:

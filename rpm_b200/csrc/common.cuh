@@ -181,7 +181,8 @@ struct CubeView {
   // complex64 views of shapes with shape-specialised passes: per outer index
   // the merged diagonal / electron-flip records of pass R (outer digits
   // 0..K-3 of the right radical) and pass L (0..K-4 of the left), laid out as
-  // {float d[2]; float2 f[2]} (24 bytes) and padded to 16 bytes; else null
+  // {float d[2]; float2 f[2]} (24 bytes) and padded to 16 bytes, the pass-L
+  // records followed by the 16 float2 of the pair operator; else null
   const void* orecR;
   const void* orecL;
   int orec_bytes_r, orec_bytes_l;

@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(PassL<T, N1, NH>::WARPS * 32, FastT<T>::MINB)
   const bool store = !fused || !a.lz.last;
   const R sf = a.lz.on ? R(1) : (R)in_scale(a, b);  // fused / Arnoldi: pass R wrote the scaled v_j
   double dot = 0.0, nw = 0.0, nv = 0.0;
-  l_tile_math<T, N1, NH>(tab, orec, tile, view, c0, quarter, yb + (long long)b * (a.ya_ld ? a.ya_ld : a.ld),
+  l_tile_math<T, N1, NH>(tab, orec, tile, view->pair, HR, c0, quarter, yb + (long long)b * (a.ya_ld ? a.ya_ld : a.ld),
                          a.out + (long long)b * a.ld, sf, store, threadIdx.x >> 5, P::WARPS, dot, nw, nv);
   if constexpr (EPU == 2) {
     if (fused) finish_lanczos(a, b, dot, nw, nv);

@@ -321,10 +321,12 @@ __device__ __forceinline__ void r_tile_math(const T* tab, const ORec<T>* orec, c
 
 // Pass-L arithmetic of one staged tile: columns c0 .. c0 + 7 of both
 // electron-B halves of vector b, staged at `tile` (16 elements per l); adds
-// the pass-R partial y_vec and writes out_vec (when `store`).  Accumulates
-// sf <x, out>, |out|^2 and |x|^2 over its elements (x: the staged input).
+// the pass-R partial y_vec and writes out_vec (when `store`).  `pair` is the
+// 4 x 4 electron-pair operator, HR the right radical's half size.
+// Accumulates sf <x, out>, |out|^2 and |x|^2 over its elements (x: the staged
+// input).
 template <class T, int N1, int NH>
-__device__ __forceinline__ void l_tile_math(const T* tab, const ORec<T>* orec, const T* tile, const CubeView<T>* view,
+__device__ __forceinline__ void l_tile_math(const T* tab, const ORec<T>* orec, const T* tile, const T* pair, int HR,
                                             int c0, long long quarter, const T* y_vec, T* out_vec,
                                             typename FastT<T>::R sf, bool store, int warp, int nwarps, double& dot,
                                             double& nw, double& nv) {
@@ -333,7 +335,6 @@ __device__ __forceinline__ void l_tile_math(const T* tab, const ORec<T>* orec, c
   using R = typename FastT<T>::R;
   constexpr int K = S::K;
   constexpr int HL = P::HL, NO = P::NO;
-  const int HR = view->half_r;
   const int lane = threadIdx.x & 31;
   const int j = lane & 7, h = (lane >> 3) & 1, lg = lane >> 4, c = lane & 15;
   // electron-pair operator rows of (e, h): eB-diagonal part merged, eB flip via the partner column
@@ -341,10 +342,10 @@ __device__ __forceinline__ void l_tile_math(const T* tab, const ORec<T>* orec, c
   T fp[2], pp[2][2];
 #pragma unroll
   for (int e = 0; e < 2; ++e) {
-    dp[e] = view->pair[(e * 2 + h) * 4 + e * 2 + h].x;
-    fp[e] = view->pair[(e * 2 + h) * 4 + (1 - e) * 2 + h];
+    dp[e] = pair[(e * 2 + h) * 4 + e * 2 + h].x;
+    fp[e] = pair[(e * 2 + h) * 4 + (1 - e) * 2 + h];
 #pragma unroll
-    for (int ep = 0; ep < 2; ++ep) pp[e][ep] = view->pair[(e * 2 + h) * 4 + ep * 2 + (1 - h)];
+    for (int ep = 0; ep < 2; ++ep) pp[e][ep] = pair[(e * 2 + h) * 4 + ep * 2 + (1 - h)];
   }
   // lane digit K-3
   R dL[2];
@@ -361,11 +362,11 @@ __device__ __forceinline__ void l_tile_math(const T* tab, const ORec<T>* orec, c
   cube_consts<S>(tab, din, fin);
   // imaginary diagonal of the pair operator: nonzero only with unequal
   // recombination rates (the non-Hermitian -(i/2) |kS - kT| Q term)
-  const bool cdiag = view->pair[0].y != R(0) || view->pair[5].y != R(0) || view->pair[10].y != R(0) ||
-                     view->pair[15].y != R(0);
+  const bool cdiag = pair[0].y != R(0) || pair[5].y != R(0) || pair[10].y != R(0) ||
+                     pair[15].y != R(0);
   R gim[2];
 #pragma unroll
-  for (int e = 0; e < 2; ++e) gim[e] = view->pair[(e * 2 + h) * 4 + e * 2 + h].y;
+  for (int e = 0; e < 2; ++e) gim[e] = pair[(e * 2 + h) * 4 + e * 2 + h].y;
   const T* col = tile + c;
   const long long cofs = h * quarter + c0 + j;
   const T* y_b = y_vec + cofs;

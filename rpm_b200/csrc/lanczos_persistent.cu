@@ -163,7 +163,9 @@ struct PShape {
   static_assert(HL % LSPLIT == 0, "l extent must split into equal tensor boxes");
   static_assert(HR % 8 == 0, "pass L tiles need 8 | HR");
   static constexpr int TAB_BYTES = align128c(cmax(SR::NTAB, SL::NTAB) * 8);
-  static constexpr int OREC_BYTES = align128c(cmax(PR::NO, PL::NO) * (int)sizeof(ORec<float2>));
+  // outer records (pass R), or outer records + the 128-byte pair operator (pass L)
+  static constexpr int OREC_BYTES =
+      align128c(cmax((PR::NO * 24 + 15) / 16 * 16, (PL::NO * 24 + 15) / 16 * 16 + 128));
   static constexpr int R_TILE_BYTES = TR * PR::RS * 8;  // one padded R tile
   static constexpr int L_TILE_BYTES = 2 * HL * 16 * 8;
   static constexpr int TILE_BYTES = align128c(cmax(2 * R_TILE_BYTES, L_TILE_BYTES));
@@ -174,6 +176,7 @@ struct PShape {
 struct Item {
   int kind;  // 0: R, 1: L, -1: end
   int j, b, tile, skip;
+  float al, sc, bp;  // R with j > 0: alpha_{j-1}, 1 / beta_{j-1}, beta_{j-1}
 };
 
 // Item index -> (phase, iteration within the launch, vector, tile) in the
@@ -246,7 +249,7 @@ __global__ void __maxnreg__(PRegs<CW>::value)
   constexpr int HL = PS::HL, HR = PS::HR, TR = PS::TR, RS = PR::RS;
   constexpr long long QUARTER = (long long)HL * HR;
   constexpr int OREC_R = ((PR::NO * 24) + 15) / 16 * 16;
-  constexpr int OREC_L = ((PL::NO * 24) + 15) / 16 * 16;
+  constexpr int OREC_L = ((PL::NO * 24) + 15) / 16 * 16 + 128;  // + the pair operator
   static_assert(OREC_R <= PS::OREC_BYTES && OREC_L <= PS::OREC_BYTES, "outer records exceed their stage slot");
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base =
@@ -326,22 +329,34 @@ __global__ void __maxnreg__(PRegs<CW>::value)
         if (lane == 0) {
           const int need = m.kind == 0 ? 2 * m.j : 2 * m.j + 1;
           if (need > 0) ok = wait_progress(p.prog + m.b, need, p.status);
+          if (ok) {
+            // per-vector scalars published with the progress this item waited
+            // for: the consumers take them from the item record
+            m.skip = *reinterpret_cast<volatile int*>(p.skip + (long long)m.b * p.istride) != 0;
+            if (m.kind == 0 && m.j > 0) {
+              const long long d = (long long)m.b * p.dstride;
+              m.al = (float)__ldcg(p.alpha + d + m.j - 1);
+              m.sc = (float)__ldcg(p.scale + d);
+              m.bp = (float)__ldcg(p.beta + d + m.j - 1);
+            }
+          }
         }
         ok = __shfl_sync(0xffffffffu, ok, 0);
+        m.skip = __shfl_sync(0xffffffffu, m.skip, 0);
         if (!ok) m.kind = -1;
       }
       armed_use[s] = use;
-      armed_copies[s] = m.kind >= 0;
-      if (m.kind < 0) {
+      armed_copies[s] = m.kind >= 0 && !m.skip;
+      if (m.kind < 0 || m.skip) {
+        // the end, or a vector that stopped: no data, the record only
         if (lane == 0) {
           meta[s] = m;
           mbar_arrive(&full_bar[s]);
         }
         __syncwarp();
-        break;
+        if (m.kind < 0) break;
+        continue;
       }
-      // stage the item's data (also for a vector that stopped: the consumers
-      // read its skip flag and leave the staged data unused)
       fence_proxy_async();
       const void* ptrs[4];
       view_ptrs(m.b, ptrs);
@@ -479,10 +494,9 @@ __global__ void __maxnreg__(PRegs<CW>::value)
       break;
     }
     // a vector stopped by a breakdown (or finished before this Krylov step)
-    // keeps its counters moving but does no arithmetic; the flag was set
-    // before the progress this item waited for
-    const bool skip = *reinterpret_cast<volatile int*>(p.skip + (long long)m.b * p.istride) != 0;
-    m.skip = skip ? 1 : 0;
+    // keeps its counters moving but does no arithmetic (the producer read the
+    // flag after the progress this item waited for)
+    const bool skip = m.skip != 0;
     bool ok = true;
     if (!skip) {
       float2* tab = stage_tab(s);
@@ -499,9 +513,8 @@ __global__ void __maxnreg__(PRegs<CW>::value)
         float bprev = 0.0f;
         if (prev) {
           // v_j = (w'_j - alpha_{j-1} v_{j-1}) / beta_{j-1}: into the tile and the basis
-          const float al = (float)p.alpha[(long long)b * p.dstride + m.j - 1];
-          const float sc = (float)p.scale[(long long)b * p.dstride];
-          bprev = (float)p.beta[(long long)b * p.dstride + m.j - 1];
+          const float al = m.al, sc = m.sc;
+          bprev = m.bp;
           constexpr int CH = HR / 2;  // 16-byte units per half row
           for (int u = tid; u < rows * 2 * CH; u += kConsumers) {
             const int rr = u / (2 * CH), rem = u - rr * (2 * CH);
@@ -530,9 +543,9 @@ __global__ void __maxnreg__(PRegs<CW>::value)
           r_tile_math<float2, N1R, NHR>(tab, orec, tile, ptile, rows, row0, HL, QUARTER, yb, 1.0f, bprev, prev, warp,
                                         CW);
       } else {
-        const CubeView<float2>* view = p.views + (p.sys_of ? p.sys_of[b] : 0);
+        const float2* pair = reinterpret_cast<const float2*>(reinterpret_cast<const char*>(orec) + OREC_L - 128);
         double dot = 0.0, nw = 0.0, nv = 0.0;
-        l_tile_math<float2, N1L, NHL>(tab, orec, tile, view, m.tile * 8, QUARTER, yb, vj + p.ld, 1.0f,
+        l_tile_math<float2, N1L, NHL>(tab, orec, tile, pair, HR, m.tile * 8, QUARTER, yb, vj + p.ld, 1.0f,
                                       m.j < p.m - 1, warp, CW, dot, nw, nv);
         dot = warp_sum_d(dot);
         nw = warp_sum_d(nw);

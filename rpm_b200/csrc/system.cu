@@ -307,11 +307,16 @@ static void upload_system(rpm_system* sys) {
       const CubeSide& cr = sys->cube_r;
       if (c32.inner_r >= 2 && c32.inner_l >= 3 && cr.half % 4 == 0 && cl.half % 8 == 0) {
         const std::vector<float> rr = outer_records(cr, tr32, cr.K - 2, 4);
-        const std::vector<float> rl = outer_records(cl, tl32, cl.K - 3, 8);
+        std::vector<float> rl = outer_records(cl, tl32, cl.K - 3, 8);
+        // the electron-pair operator follows the pass-L records (staged together)
+        for (int k = 0; k < 16; ++k) {
+          rl.push_back(c32.pair[k].x);
+          rl.push_back(c32.pair[k].y);
+        }
         c32.orecR = upload<float>(sys, rr.data(), rr.size() * sizeof(float));
         c32.orecL = upload<float>(sys, rl.data(), rl.size() * sizeof(float));
         c32.orec_bytes_r = (int)(rr.size() * sizeof(float));
-        c32.orec_bytes_l = (int)(rl.size() * sizeof(float));
+        c32.orec_bytes_l = (int)(rl.size() * sizeof(float));  // records (padded to 16 bytes) + 128 pair bytes
       }
       sys->cube64_dev = upload<CubeView<double2>>(sys, &c64, sizeof(c64));
       sys->cube32_dev = upload<CubeView<float2>>(sys, &c32, sizeof(c32));
@@ -553,6 +558,13 @@ int rpm_system_set_recombination(rpm_system* sys, double singlet_rate, double tr
         sys->split32.pair[k] = make_float2((float)v.x, (float)v.y);
         sys->cube64.pair[k] = v;
         sys->cube32.pair[k] = make_float2((float)v.x, (float)v.y);
+      }
+      if (sys->cube && sys->cube32.orecL) {
+        // the copy of the pair operator that follows the pass-L outer records
+        float2 pair32[16];
+        for (int k = 0; k < 16; ++k) pair32[k] = sys->cube32.pair[k];
+        char* dst = static_cast<char*>(const_cast<void*>(sys->cube32.orecL)) + sys->cube32.orec_bytes_l - sizeof(pair32);
+        rpm::check_cuda(cudaMemcpy(dst, pair32, sizeof(pair32), cudaMemcpyHostToDevice), "update pair operator");
       }
       if (sys->cube) {
         rpm::check_cuda(cudaMemcpy(sys->cube64_dev, &sys->cube64, sizeof(sys->cube64), cudaMemcpyHostToDevice),

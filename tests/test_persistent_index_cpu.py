@@ -41,7 +41,9 @@ class PShape:
         assert self.HL % self.LSPLIT == 0 and self.HR % 8 == 0
         self.NTAB_R, self.NTAB_L = ntab(n1r, nhr), ntab(n1l, nhl)
         self.TAB_BYTES = align128(max(self.NTAB_R, self.NTAB_L) * 8)
-        self.OREC_BYTES = align128(max(self.HR // 4, self.HL // 8) * ORREC)
+        self.OREC_R = (self.HR // 4 * ORREC + 15) // 16 * 16
+        self.OREC_L = (self.HL // 8 * ORREC + 15) // 16 * 16 + 128  # + the pair operator
+        self.OREC_BYTES = align128(max(self.OREC_R, self.OREC_L))
         self.R_TILE = self.TR * self.RS * 8
         self.L_TILE = 2 * self.HL * 16 * 8
         self.TILE_BYTES = align128(max(2 * self.R_TILE, self.L_TILE))
@@ -101,10 +103,10 @@ def test_stage_layout_and_copy_addresses(shape):
     for nt in (ps.NTAB_R, ps.NTAB_L):
         assert nt * 8 % 16 == 0 and nt * 8 <= ps.TAB_BYTES
     assert max(ps.HR // 4, ps.HL // 8) * ORREC <= ps.OREC_BYTES
-    # outer-index records: one bulk copy each, padded to 16 bytes, inside the slot
-    for no in (ps.HR // 4, ps.HL // 8):
-        padded = (no * ORREC + 15) // 16 * 16
-        assert padded % 16 == 0 and padded <= ps.OREC_BYTES
+    # outer-index records (pass L: + the 128-byte pair operator): one bulk copy
+    # each, a multiple of 16 bytes, inside the slot
+    for size in (ps.OREC_R, ps.OREC_L):
+        assert size % 16 == 0 and size <= ps.OREC_BYTES
     ld = (ps.N + 63) // 64 * 64
     m = 40
     vstride = (m + 1) * ld
