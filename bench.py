@@ -462,8 +462,17 @@ def b200_arm(args, rank: int, world: int, dist) -> None:
                       reorth_periods=(0, 16), lanczos_kernel=args.lanczos)
         krylov, tile, reorth = tuning.krylov_dimension, tuning.tile, tuning.reorth_period
     krylov = int(krylov)
-    bp = BatchedPropagator(hams, krylov_dimension=krylov, state_error_budget=budget, lanczos_kernel=args.lanczos,
-                           wavefront=args.wavefront, reorth_period=reorth)
+    knobs = dict(krylov_dimension=krylov, state_error_budget=budget, lanczos_kernel=args.lanczos,
+                 wavefront=args.wavefront, reorth_period=reorth)
+    if args.parts > 1:
+        # independent halves of the step on two streams: one half's controller,
+        # Gram and rebuild run beside the other half's persistent Lanczos launch
+        from rpm_b200.batched import ConcurrentBatches
+
+        bp = ConcurrentBatches(hams, parts=args.parts, reserve_sms=args.reserve_sms, **knobs)
+        tile = ntraj
+    else:
+        bp = BatchedPropagator(hams, **knobs)
     ld = bp.leading_dimension
     pristine = torch.zeros((ntraj, ld), dtype=torch.complex128, device=dev)
     pristine[:, :n].copy_(torch.from_numpy(states))
@@ -544,16 +553,17 @@ def b200_arm(args, rank: int, world: int, dist) -> None:
         iter_s = counters["hpsi_ms"] / 1e3
         persistent = kind == "persistent"
         iters = krylov if persistent else 1
-        alg_bytes = 32.0 * n * tile * iters
+        per_launch = tile // max(1, args.parts)  # trajectories of one launch
+        alg_bytes = 32.0 * n * per_launch * iters
         launch_s = iter_s * iters
         achieved = alg_bytes / launch_s / 1e9 if launch_s > 0 else None
         per_vec_iter = ncu_traffic_per_vector_iteration() if persistent else ncu_traffic_per_vector(True)
-        kernel = (f"k_lanczos_persistent<2,5,1,6> (all {krylov} Lanczos iterations of a Krylov step for {tile} "
+        kernel = (f"k_lanczos_persistent<2,5,1,6> (all {krylov} Lanczos iterations of a Krylov step for {per_launch} "
                   "trajectories: complex64 H psi + Paige 3-term recurrence, TMA-staged)" if persistent else
                   "fast_pass_r + fast_pass_l (one fused Lanczos iteration, all trajectories)")
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak if achieved else None,
-                    "traffic": per_vec_iter * tile * iters if per_vec_iter is not None else None,
+                    "traffic": per_vec_iter * per_launch * iters if per_vec_iter is not None else None,
                     "traffic_source": ("profiles/lanczos_persistent_c64.md (ncu capture of this kernel; command "
                                        "there), scaled to one launch" if persistent else
                                        "profiles/lanczos_iteration_fused_c64.md"),
@@ -602,6 +612,7 @@ def b200_arm(args, rank: int, world: int, dist) -> None:
             "config": {"workload": WORKLOAD, "batch": f"{args.orientations} Fibonacci field orientations x {nvec} "
                                                       "random-phase vectors per GPU per step",
                        "trajectories_per_step_per_gpu": per_rank, "krylov_dim": krylov, "tile": tile,
+                       "concurrent_parts": args.parts,
                        "reorth_period": reorth, "lanczos_kernel": kind,
                        "tuning": ("autotuned: Krylov " + str(list(KRYLOV_RANGE)) + ", tile, reorthogonalisation "
                                   "(none / 16), accuracy-gated" if tuning else "fixed"),
@@ -640,6 +651,10 @@ def main() -> None:
     p.add_argument("--lanczos", choices=("persistent", "passes"), default="persistent",
                    help="Lanczos iterations of a Krylov step: one persistent launch, or two pass launches each")
     p.add_argument("--wavefront", type=int, default=0, help="persistent kernel: vectors per wavefront group (0: 12)")
+    p.add_argument("--parts", type=int, default=1,
+                   help="run the step's trajectories as this many concurrent batches on their own streams")
+    p.add_argument("--reserve-sms", type=int, default=16,
+                   help="with --parts > 1: SMs each persistent launch leaves to the other batch's kernels")
     p.add_argument("--persistent-warps", type=int, choices=(8, 10), default=8,
                    help="persistent kernel: consumer warps per CTA")
     p.add_argument("--reorth-period", type=int, default=0,

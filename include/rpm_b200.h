@@ -257,6 +257,10 @@ typedef struct rpm_batch_config {
                                   basis (two classical Gram-Schmidt passes,
                                   FP64 sums over the complex64 basis)        */
   int reorth_period;           /* iterations between reorthogonalisations    */
+  int persistent_ctas;         /* CTAs of a persistent launch (<=0: one per
+                                  SM); fewer leave SMs free for the other
+                                  kernels of a batch running concurrently on
+                                  another stream                             */
 } rpm_batch_config;
 
 #define RPM_LANCZOS_PERSISTENT 0

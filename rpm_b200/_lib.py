@@ -56,7 +56,8 @@ class rpm_batch_config(ctypes.Structure):
                 ("maximum_step_us", ctypes.c_double), ("minimum_step_us", ctypes.c_double),
                 ("breakdown_relative", ctypes.c_double), ("use_graph", ctypes.c_int),
                 ("max_steps", ctypes.c_longlong), ("lanczos_kernel", ctypes.c_int), ("wavefront", ctypes.c_int),
-                ("reorth_policy", ctypes.c_int), ("reorth_period", ctypes.c_int)]
+                ("reorth_policy", ctypes.c_int), ("reorth_period", ctypes.c_int),
+                ("persistent_ctas", ctypes.c_int)]
 
 
 class rpm_batch_stats(ctypes.Structure):

@@ -64,14 +64,17 @@ class BatchedPropagator:
     ``reorth_period`` > 0 reorthogonalises the next Lanczos vector against the
     whole basis after every that many iterations (two classical Gram-Schmidt
     passes in FP64 over the complex64 basis); 0 keeps the plain three-term
-    recurrence.
+    recurrence.  ``persistent_ctas`` > 0 limits a persistent launch to that
+    many CTAs (one per SM otherwise), leaving SMs to another batch that runs
+    concurrently on its own stream.
     """
 
     def __init__(self, hamiltonians: Sequence[MatrixFreeHamiltonian], *, krylov_dimension: int = 32,
                  embedded_offset: int = 4, safety_factor: float = 2.0, state_error_budget: float = 1e-7,
                  initial_step_us: float = 0.05, maximum_step_us: float = 0.25, minimum_step_us: float = 1e-9,
                  breakdown_relative: float = 1e-5, use_graph: bool = True, max_steps: int = 0,
-                 lanczos_kernel: str = "passes", wavefront: int = 0, reorth_period: int = 0) -> None:
+                 lanczos_kernel: str = "persistent", wavefront: int = 0, reorth_period: int = 0,
+                 persistent_ctas: int = 0) -> None:
         hams = list(hamiltonians)
         if not hams:
             raise ValueError("At least one Hamiltonian is required.")
@@ -98,6 +101,7 @@ class BatchedPropagator:
             raise ValueError("reorth_period must be >= 0")
         cfg.reorth_policy = 1 if int(reorth_period) > 0 else 0
         cfg.reorth_period = int(reorth_period)
+        cfg.persistent_ctas = int(persistent_ctas)
         self.config = cfg
         handles = (ctypes.c_void_p * len(hams))(*[h._system.handle.value for h in hams])
         handle = ctypes.c_void_p()
@@ -371,3 +375,116 @@ def propagate_segments_batched(initial_states, times_us, segments: Sequence[Batc
                                 float(min_step[b]) if np.isfinite(min_step[b]) else 0.0, float(max_step[b]),
                                 float(accumulated[b]), 0.0) for b in range(ntraj))
     return BatchedResult(times, values, bounds, errors, yields, psi, st, np.zeros(ntraj, dtype=np.int32))
+
+
+class ConcurrentBatches:
+    """Trajectories split into ``parts`` independent batches that run on their
+    own streams at the same time (one host thread per part).
+
+    Each part is a :class:`BatchedPropagator` whose persistent Lanczos launches
+    leave ``reserve_sms`` SMs free, so that while one part runs its Lanczos
+    iterations the other's controller, Gram, rebuild and observation kernels
+    run on the free SMs instead of waiting.  Results are those of the parts
+    (same arithmetic per trajectory) in the caller's order.
+    """
+
+    def __init__(self, hamiltonians: Sequence[MatrixFreeHamiltonian], *, parts: int = 2, reserve_sms: int = 16,
+                 **knobs) -> None:
+        torch = _torch()
+        if parts < 1:
+            raise ValueError("parts must be positive")
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+        ctas = max(1, sms - int(reserve_sms)) if parts > 1 else 0
+        self.parts = [BatchedPropagator(hamiltonians, persistent_ctas=ctas, **knobs) for _ in range(parts)]
+        self.streams = [torch.cuda.Stream() for _ in range(parts)]
+        self.hamiltonians = self.parts[0].hamiltonians
+        self.leading_dimension = self.parts[0].leading_dimension
+
+    def _spans(self, n: int):
+        k = len(self.parts)
+        edges = [round(i * n / k) for i in range(k + 1)]
+        return [(edges[i], edges[i + 1]) for i in range(k) if edges[i + 1] > edges[i]]
+
+    def propagate_device(self, psi, times_us, system_index):
+        """As :meth:`BatchedPropagator.propagate_device` on a (trajectories, ld)
+        buffer; the parts take contiguous row blocks."""
+        import threading
+
+        torch = _torch()
+        idx = np.ascontiguousarray(system_index, dtype=np.int32)
+        spans = self._spans(idx.size)
+        out = [None] * len(spans)
+        errors = []
+        caller = torch.cuda.current_stream()
+
+        def run(k, a, b):
+            try:
+                s = self.streams[k]
+                s.wait_stream(caller)
+                with torch.cuda.stream(s):
+                    out[k] = self.parts[k].propagate_device(psi[a:b], times_us, idx[a:b], stream=s)
+            except Exception as exc:  # re-raised in the caller
+                errors.append(exc)
+
+        threads = [threading.Thread(target=run, args=(k, a, b)) for k, (a, b) in enumerate(spans)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        if errors:
+            raise errors[0]
+        for s in self.streams[: len(spans)]:
+            caller.wait_stream(s)
+        values = torch.cat([o[0] for o in out])
+        errs = torch.cat([o[1] for o in out])
+        stats = [st for o in out for st in o[2]]
+        return values, errs, stats
+
+    def counters(self, reset: bool = False) -> dict:
+        got = [p.counters(reset) for p in self.parts]
+        n = sum(g["hpsi_samples"] for g in got)
+        return {"kernel_launches": sum(g["kernel_launches"] for g in got),
+                "step_replays": sum(g["step_replays"] for g in got),
+                "hpsi_ms": sum(g["hpsi_ms"] * g["hpsi_samples"] for g in got) / n if n else 0.0,
+                "hpsi_samples": n}
+
+    def lanczos_kind(self) -> str:
+        return self.parts[0].lanczos_kind()
+
+    def yields_device(self, times_us, values, lifetime_us: float):
+        return self.parts[0].yields_device(times_us, values, lifetime_us)
+
+    def propagate(self, initial_states, times_us, *, system_index=None, lifetime_us=None):
+        """The public path from host states: per part :meth:`BatchedPropagator.propagate`
+        (host to device copies included), concurrently, results concatenated."""
+        import threading
+
+        n = len(initial_states)
+        idx = np.zeros(n, dtype=np.int32) if system_index is None else np.asarray(system_index, dtype=np.int32)
+        spans = self._spans(n)
+        out = [None] * len(spans)
+        errors = []
+
+        def run(k, a, b):
+            try:
+                torch = _torch()
+                with torch.cuda.stream(self.streams[k]):
+                    out[k] = self.parts[k].propagate(initial_states[a:b], times_us, system_index=idx[a:b],
+                                                     lifetime_us=lifetime_us)
+                self.streams[k].synchronize()
+            except Exception as exc:
+                errors.append(exc)
+
+        threads = [threading.Thread(target=run, args=(k, a, b)) for k, (a, b) in enumerate(spans)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        if errors:
+            raise errors[0]
+        cat = np.concatenate
+        return BatchedResult(out[0].times_us, cat([o.observable_values for o in out]),
+                             cat([o.observable_error_bounds for o in out]),
+                             cat([o.state_error_estimates for o in out]),
+                             None if out[0].yields is None else cat([o.yields for o in out]), None,
+                             tuple(s for o in out for s in o.stats), cat([o.status for o in out]))

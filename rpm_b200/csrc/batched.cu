@@ -1448,6 +1448,7 @@ static void record_step(rpm_batch* Bh, const BatchDev& B, const Layout& L, cudaS
       P.part_stride = B.ppart_stride;
       P.work = B.work + g * nseg + seg;
       P.status = B.kstatus;
+      P.ctas = Bh->cfg.persistent_ctas;
       if (!launch_lanczos_persistent(P, G.plan, B.V, (long long)B.ntraj * (m + 1), st))
         fail(RPM_E_INVALID, "persistent Lanczos kernel unavailable");
     }

@@ -101,6 +101,7 @@ struct PersistentLanczos {
   int part_stride;
   unsigned* work;  // dequeue counter of this launch
   int* status;     // sticky wait-timeout flag
+  int ctas;        // CTAs of the launch (<= 0: one per SM)
 };
 
 // Launches the persistent Lanczos kernel for the plan's shape; false (nothing

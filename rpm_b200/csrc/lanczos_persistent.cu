@@ -31,6 +31,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 #include <string>
@@ -630,7 +631,8 @@ void launch_instance(const PersistentLanczos& p, const float2* V_base, long long
     }
   }
   const CUtensorMap map = basis_map<PS>(V_base, nslots, p.ld);
-  kern<<<sm_count(), kThreads, PS::SMEM, st>>>(map, p);
+  const int ctas = p.ctas > 0 ? std::min(p.ctas, sm_count()) : sm_count();
+  kern<<<ctas, kThreads, PS::SMEM, st>>>(map, p);
   check_launch("k_lanczos_persistent");
 }
 

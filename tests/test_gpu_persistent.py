@@ -108,3 +108,30 @@ def test_periodic_reorthogonalisation(period):
     for k in range(nvec):
         _, y_ref = _plain_yield(rb, hams[index[k]], states[k], times, sub.dimensions)
         assert abs(out["persistent"].yields[k] - y_ref) < YIELD_TOL
+
+
+def test_concurrent_batches_match_one_batch():
+    """Two concurrent batches on their own streams (persistent launches that
+    leave SMs free) give the single batch's results trajectory by trajectory."""
+    import torch
+
+    from rpm_b200 import synthetic
+    from rpm_b200.batched import BatchedPropagator, ConcurrentBatches
+
+    sub, hams = _systems("prefix", 3)
+    nvec = 9
+    states = synthetic.random_phase_vectors(sub.dimensions, nvec, 41)
+    index = np.arange(nvec) % len(hams)
+    times = np.arange(81) * 0.00125
+    one = BatchedPropagator(hams, krylov_dimension=16, state_error_budget=1e-8)
+    two = ConcurrentBatches(hams, parts=2, reserve_sms=16, krylov_dimension=16, state_error_budget=1e-8)
+    ref = one.propagate(list(states), times, system_index=index, lifetime_us=1.0)
+    got = two.propagate(list(states), times, system_index=index, lifetime_us=1.0)
+    assert np.max(np.abs(got.observable_values - ref.observable_values)) < SAME_TOL
+    assert np.max(np.abs(got.yields - ref.yields)) < SAME_TOL
+    # the device-buffer path of the benchmark
+    psi = one.load_states(list(states), index)
+    v1, _, _ = one.propagate_device(psi.clone(), times, index)
+    v2, _, _ = two.propagate_device(psi.clone(), times, index)
+    torch.cuda.synchronize()
+    assert float(torch.max(torch.abs(v1 - v2))) < SAME_TOL
