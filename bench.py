@@ -348,57 +348,109 @@ def adjoint_sample(full, direction, dev, vectors: int = 16, horizon_us: float = 
     return out
 
 
-def uneven_sample(args) -> dict:
-    """Uneven system sizes with unequal recombination rates in one propagate
-    call: equal-count nuclear prefixes of 3, 5 and 7 nuclei per radical (864,
-    13,824 and 221,184 dimensions), kS = 1e6 and kT = 2e6 s^-1, trajectories
-    split 16 : 10 : 6 (the 512 : 320 : 192 proportions at 1/32 scale), field
-    directions from a 64 x 32 (theta, phi) grid, Arnoldi per shape group."""
+UNEVEN_COUNTS = {3: 512, 5: 320, 7: 192}  # nuclei per radical -> trajectories (864 / 13,824 / 221,184 dims)
+
+
+def uneven_sample(args, scale: float = 1.0, horizon_us: float = HORIZON_US) -> dict:
+    """Uneven system sizes with unequal recombination rates, mixed in every
+    launch: equal-count nuclear prefixes of 3, 5 and 7 nuclei per radical (6,
+    10 and 14 nuclei; 864, 13,824 and 221,184 dimensions), kS = 1e6 and
+    kT = 2e6 s^-1, trajectories split 512 : 320 : 192 (times ``scale``), each
+    with its own field direction drawn without repetition from a 64 x 32
+    (theta, phi) grid at 50 uT and its own random-phase vector, to
+    ``horizon_us``.  Each shape group is autotuned alone on a 0.25-us prefix
+    (Krylov dimension 16-40 and tile, accuracy-gated); the group's dimension
+    becomes its systems' Krylov cap in the mixed batch, and each launch
+    carries at most one tile of every group.  Timed end to end through
+    ``propagate`` (host states in, yields out); a tight-budget rerun of two
+    trajectories per group at the batch's largest dimension checks the yields."""
     import numpy as np
     import torch
 
     import rpm_b200 as rb
     from rpm_b200 import synthetic
+    from rpm_b200.autotune import KRYLOV_RANGE, tune_per_shape
     from rpm_b200.batched import BatchedPropagator
 
     full = synthetic.full_system()
-    counts = {3: 16, 5: 10, 7: 6}
+    counts = {per: max(2, int(round(c * scale))) for per, c in UNEVEN_COUNTS.items()}
     grid = [(math.pi * (i + 0.5) / 64, 2 * math.pi * j / 32) for i in range(64) for j in range(32)]
     rng = np.random.default_rng(404)
-    hams, states, index, dims = [], [], [], []
+    pick = rng.permutation(len(grid))
+    hams, states, dims, group_pos = [], [], [], []
+    t_setup = time.perf_counter()
     for per, count in counts.items():
         sub = synthetic.prefix_system(full, per) if per < 7 else full
-        for t in range(count):
-            th, ph = grid[int(rng.integers(len(grid)))]
+        pos = []
+        for _ in range(count):
+            th, ph = grid[int(pick[len(hams) % len(grid)])]
             h = rb.CompiledFullPairHamiltonian(sub.dimensions, sub.terms(th, ph), left_axes=sub.left_axes,
                                                right_axes=sub.right_axes)
             h.set_recombination_rates(1.0, 2.0)
-            index.append(len(hams))
+            pos.append(len(hams))
             hams.append(h)
             states.append(synthetic.random_phase_vectors(sub.dimensions, 1, 900 + len(states))[0])
             dims.append(sub.dimension)
-    times = np.arange(int(round(args.horizon / GRID_US)) + 1) * GRID_US
-    from rpm_b200.autotune import KRYLOV_RANGE, tune
-
-    tuning = tune(hams, states, index, horizon_us=0.25, yield_tolerance=YIELD_TOL, krylov_dimensions=KRYLOV_RANGE,
-                  tiles=(len(states),))
-    bp = BatchedPropagator(hams, krylov_dimension=tuning.krylov_dimension, state_error_budget=0.5 * YIELD_TOL)
-    first = [0, counts[3], counts[3] + counts[5]]  # one trajectory of each size
+        group_pos.append(pos)
+    t_setup = time.perf_counter() - t_setup
+    index = list(range(len(hams)))
+    times = np.arange(int(round(horizon_us / GRID_US)) + 1) * GRID_US
+    # tuning sample: up to 192 trajectories of every group
+    sample = [p for pos in group_pos for p in pos[:192]]
+    t_tune = time.perf_counter()
+    tuning = tune_per_shape([hams[p] for p in sample], [states[p] for p in sample], list(range(len(sample))),
+                            horizon_us=0.25, full_horizon_us=horizon_us, yield_tolerance=YIELD_TOL,
+                            krylov_dimensions=KRYLOV_RANGE, tiles=(16, 48, 96, 192, 320, 512))
+    t_tune = time.perf_counter() - t_tune
+    group_caps = [r.krylov_dimension for r in tuning.results]
+    group_tiles = [r.tile for r in tuning.results]
+    caps = [group_caps[g] for g, pos in enumerate(group_pos) for _ in pos]
+    bp = BatchedPropagator(hams, krylov_dimension=max(caps), state_error_budget=tuning.state_error_budget,
+                           krylov_caps=caps)
+    chunks = max(-(-len(pos) // t) for pos, t in zip(group_pos, group_tiles))
+    launches = []
+    for c in range(chunks):
+        sel = []
+        for pos in group_pos:
+            per_chunk = -(-len(pos) // chunks)
+            sel += pos[c * per_chunk:(c + 1) * per_chunk]
+        launches.append(sel)
+    first = [pos[0] for pos in group_pos]
     bp.propagate([states[k] for k in first], times[:9], system_index=first)  # warm-up
     torch.cuda.synchronize()
+    yields = np.empty(len(hams))
+    stats = [None] * len(hams)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    out = bp.propagate(states, times, system_index=index)
+    for sel in launches:
+        out = bp.propagate([states[k] for k in sel], times, system_index=sel)
+        yields[sel] = out.yields
+        for k, st in zip(sel, out.stats):
+            stats[k] = st
     e1.record()
     torch.cuda.synchronize()
     seconds = e0.elapsed_time(e1) / 1e3
-    return {"probe": "uneven_sizes_unequal_rates", "trajectories": len(states), "seconds": seconds,
-            "trajectories_per_s": len(states) / seconds, "horizon_us": float(times[-1]),
-            "dimensions": {str(d): dims.count(d) for d in sorted(set(dims))},
-            "yield_range": [float(np.min(out.yields)), float(np.max(out.yields))],
-            "krylov_dim": tuning.krylov_dimension,
-            "autotune": [{k: t[k] for k in ("krylov_dimension", "throughput") if k in t} for t in tuning.trials],
-            "rates_per_us": [1.0, 2.0]}
+    # tight-budget check of two trajectories per group
+    check = [p for pos in group_pos for p in pos[:2]]
+    tight = BatchedPropagator([hams[k] for k in check], krylov_dimension=max(KRYLOV_RANGE),
+                              state_error_budget=tuning.state_error_budget / 100.0).propagate(
+        [states[k] for k in check], times, system_index=list(range(len(check))))
+    err = np.abs(tight.yields - yields[check])
+    per_group = []
+    for g, pos in enumerate(group_pos):
+        per_group.append({"dimension": dims[pos[0]], "trajectories": len(pos), "krylov_cap": group_caps[g],
+                          "tile": group_tiles[g],
+                          "accepted_steps_mean": float(np.mean([stats[k].accepted_steps for k in pos])),
+                          "matvecs_mean": float(np.mean([stats[k].matvecs for k in pos])),
+                          "yield_range": [float(yields[pos].min()), float(yields[pos].max())],
+                          "tuned_throughput_traj_us_per_s": tuning.results[g].throughput})
+    return {"workload": "uneven sizes 864 / 13,824 / 221,184 with kS = 1e6, kT = 2e6 s^-1 (Arnoldi), "
+                        "64 x 32 direction grid, one launch mixes every size",
+            "trajectories": len(hams), "horizon_us": float(times[-1]), "seconds": seconds,
+            "trajectories_per_s": len(hams) / seconds, "launches": chunks, "timed": "propagate (host in, yields out)",
+            "groups": per_group, "state_error_budget": tuning.state_error_budget,
+            "yield_err_vs_tight_budget": {"max": float(err.max()), "trajectories": len(check)},
+            "setup_s": t_setup, "tune_s": t_tune, "rates_per_us": [1.0, 2.0]}
 
 
 def ncu_traffic_per_vector_iteration():
@@ -607,6 +659,9 @@ def b200_arm(args, rank: int, world: int, dist) -> None:
         adjoint = None
         if world == 1 and not args.no_adjoint:
             adjoint = adjoint_sample(full, dirs[0], dev)
+        uneven = None
+        if world == 1 and not args.no_uneven:
+            uneven = uneven_sample(args, args.uneven_scale)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
@@ -633,6 +688,7 @@ def b200_arm(args, rank: int, world: int, dist) -> None:
             "yield_err_vs_fp64": y_err,
             "yields_gathered": int(yields_all.numel()),
             "adjoint": adjoint,
+            "uneven_sizes": uneven,
         }
     if line is not None:
         print(json.dumps(line), flush=True)
@@ -670,7 +726,10 @@ def main() -> None:
                    help="plain FP64 trajectories (vector 0 of that many orientations) for the yield errors")
     p.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-gradient side measurement")
     p.add_argument("--uneven", action="store_true",
-                   help="diagnostic: uneven sizes (864 / 13,824 / 221,184) with unequal rates, --horizon us")
+                   help="only the uneven-size side measurement (864 / 13,824 / 221,184 with unequal rates)")
+    p.add_argument("--uneven-scale", type=float, default=1.0,
+                   help="uneven-size side measurement: trajectory counts as a fraction of 512 / 320 / 192")
+    p.add_argument("--no-uneven", action="store_true", help="skip the uneven-size side measurement")
     p.add_argument("--adjoint-only", action="store_true",
                    help="diagnostic: only the adjoint side measurement (--vectors trajectories, --horizon us)")
     p.add_argument("--horizon", type=float, default=HORIZON_US,
@@ -684,7 +743,7 @@ def main() -> None:
         hpsi_probe(args)
         return
     if args.uneven:
-        print(json.dumps(uneven_sample(args)), flush=True)
+        print(json.dumps(uneven_sample(args, args.uneven_scale, args.horizon)), flush=True)
         return
     if args.adjoint_only:
         import torch

@@ -310,6 +310,12 @@ int rpm_batch_lanczos_kind(const rpm_batch* batch, int* kind);
 /* Consumer warps per CTA of the persistent Lanczos kernel, 8 or 10 (default
  * 8); a tuning knob for measurements, no counterpart in the reference. */
 int rpm_set_persistent_warps(int consumer_warps);
+/* Per-system Krylov dimensions (caps[k] for the batch's system k, 0: the
+ * batch's krylov_dim; otherwise 2 <= cap <= krylov_dim): a trajectory's
+ * basis ends after cap Lanczos / Arnoldi iterations, so systems of uneven
+ * size in one batch each run at their own dimension.  nsys = 0 clears them.
+ * No counterpart in the reference, whose dimension is per propagator. */
+int rpm_batch_set_krylov_caps(rpm_batch* batch, const int* caps, int nsys);
 /* Replace the configured state-error budget for later propagate calls (the
  * knob ENG:620-649 exposes as a mutable attribute). */
 int rpm_batch_set_budget(rpm_batch* batch, double state_error_budget);

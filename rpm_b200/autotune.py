@@ -203,3 +203,53 @@ def tune(hamiltonians: Sequence, states, system_index: Sequence[int], *, horizon
         stored[key] = asdict(result)
         path.write_text(json.dumps(stored, indent=1))
     return result
+
+
+@dataclass
+class ShapeTuning:
+    """Per-shape tuning of an uneven batch: each shape group's Krylov
+    dimension (the batch's per-system caps) and tile."""
+    shapes: list                      # shape key of each group, in order of first appearance
+    results: list                     # TuneResult of each group
+    caps: list                        # Krylov dimension of each Hamiltonian (its group's)
+    state_error_budget: float
+
+    @property
+    def krylov_dimension(self) -> int:
+        return max(self.caps)
+
+    def chunks(self, counts: Sequence[int]) -> int:
+        """Launches needed when each launch carries at most one tile of every group."""
+        return max(-(-int(c) // r.tile) for c, r in zip(counts, self.results))
+
+    def propagator(self, hamiltonians, **kwargs) -> BatchedPropagator:
+        reorth = max(r.reorth_period for r in self.results)
+        return BatchedPropagator(hamiltonians, krylov_dimension=self.krylov_dimension,
+                                 state_error_budget=self.state_error_budget, krylov_caps=self.caps,
+                                 reorth_period=reorth, **kwargs)
+
+
+def tune_per_shape(hamiltonians: Sequence, states, system_index: Sequence[int], *,
+                   tiles: Sequence[int] | None = None, **knobs) -> ShapeTuning:
+    """:func:`tune` run on each shape group of the sample alone (its own
+    trajectories, tiles up to its size), so that an uneven batch gives every
+    system size its own Krylov dimension and tile.  ``knobs`` are passed on to
+    :func:`tune`."""
+    hams = list(hamiltonians)
+    idx = np.asarray(system_index, dtype=np.int32)
+    shapes = [(tuple(h.dimensions), tuple(getattr(h, "left_axes", ()))) for h in hams]
+    order: list = []
+    for k in idx:
+        if shapes[int(k)] not in order:
+            order.append(shapes[int(k)])
+    results = []
+    for shape in order:
+        pos = [p for p, k in enumerate(idx) if shapes[int(k)] == shape]
+        group = sorted({int(idx[p]) for p in pos})
+        local = {k: i for i, k in enumerate(group)}
+        cand = tuple(t for t in (tiles or TILE_RANGE) if t <= len(pos)) or (len(pos),)
+        results.append(tune([hams[k] for k in group], [states[p] for p in pos],
+                            [local[int(idx[p])] for p in pos], tiles=cand, **knobs))
+    caps = [results[order.index(shapes[k])].krylov_dimension if shapes[k] in order else 0 for k in range(len(hams))]
+    return ShapeTuning(shapes=[list(map(list, s)) for s in order], results=results, caps=caps,
+                       state_error_budget=results[0].state_error_budget)

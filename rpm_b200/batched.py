@@ -66,7 +66,9 @@ class BatchedPropagator:
     passes in FP64 over the complex64 basis); 0 keeps the plain three-term
     recurrence.  ``persistent_ctas`` > 0 limits a persistent launch to that
     many CTAs (one per SM otherwise), leaving SMs to another batch that runs
-    concurrently on its own stream.
+    concurrently on its own stream.  ``krylov_caps`` gives each Hamiltonian
+    its own Krylov dimension (<= ``krylov_dimension``; 0 keeps the batch's),
+    e.g. per system size in an uneven batch.
     """
 
     def __init__(self, hamiltonians: Sequence[MatrixFreeHamiltonian], *, krylov_dimension: int = 32,
@@ -74,7 +76,7 @@ class BatchedPropagator:
                  initial_step_us: float = 0.05, maximum_step_us: float = 0.25, minimum_step_us: float = 1e-9,
                  breakdown_relative: float = 1e-5, use_graph: bool = True, max_steps: int = 0,
                  lanczos_kernel: str = "persistent", wavefront: int = 0, reorth_period: int = 0,
-                 persistent_ctas: int = 0) -> None:
+                 persistent_ctas: int = 0, krylov_caps: Sequence[int] | None = None) -> None:
         hams = list(hamiltonians)
         if not hams:
             raise ValueError("At least one Hamiltonian is required.")
@@ -110,6 +112,11 @@ class BatchedPropagator:
         ld = ctypes.c_longlong()
         _lib.call("rpm_batch_leading_dimension", handle, ctypes.byref(ld))
         self.leading_dimension = ld.value
+        if krylov_caps is not None:
+            caps = np.ascontiguousarray(krylov_caps, dtype=np.int32)
+            if caps.size != len(hams):
+                raise ValueError("krylov_caps needs one entry per Hamiltonian")
+            _lib.call("rpm_batch_set_krylov_caps", handle, _lib.iptr(caps), int(caps.size))
 
     def __del__(self):
         h = getattr(self, "_handle", None)

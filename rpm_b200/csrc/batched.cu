@@ -50,6 +50,8 @@ struct TrajState {
   int cursor, npts, done, stop, skip, msize, steps, sys;
   int status;
   int cgs_done;  // Arnoldi: the first projection kept the norm (no second pass)
+  int mcap;      // this trajectory's Krylov dimension (<= the batch's m)
+  int pad_;
 };
 static_assert(sizeof(TrajState) % 8 == 0, "TrajState must be a whole number of doubles");
 static_assert(sizeof(TrajState) % 4 == 0, "TrajState must be a whole number of ints");
@@ -126,7 +128,8 @@ __device__ __forceinline__ double2 sum_parts(const BatchDev& B, int b) {
 // ---------------------------------------------------------------------------
 // Set-up: state fields, ||psi0|| and P_S(psi0)
 // ---------------------------------------------------------------------------
-__global__ void k_b_setup(BatchDev B, const int* sys_of, const long long* n_of, double initial_step) {
+__global__ void k_b_setup(BatchDev B, const int* sys_of, const long long* n_of, const int* cap_of,
+                          double initial_step) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= B.ntraj) return;
   TrajState& s = B.st[b];
@@ -136,7 +139,8 @@ __global__ void k_b_setup(BatchDev B, const int* sys_of, const long long* n_of, 
   s.n = n_of[b];
   s.hint = initial_step;
   s.min_step = DBL_MAX;
-  s.msize = B.m;
+  s.mcap = max(2, min(B.m, cap_of[b] > 0 ? cap_of[b] : B.m));
+  s.msize = s.mcap;
   s.scale = 1.0;
   B.count[b] = 0;
 }
@@ -211,7 +215,7 @@ __global__ void __launch_bounds__(kEwThreads) k_b_start(BatchDev B) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     s.stop = 0;
     s.skip = 0;
-    s.msize = B.m;
+    s.msize = s.mcap;
     s.scale = 1.0;
   }
 }
@@ -262,7 +266,10 @@ __global__ void __launch_bounds__(kEwThreads) k_b_update(BatchDev B, int j, int 
     s.beta[j] = bj;
     s.scale = bj > 0.0 ? 1.0 / bj : 0.0;
     const double ref = fabs(s.alpha[j]) + (j > 0 ? s.beta[j - 1] : 0.0);
-    if (!(bj > B.breakdown_rel * ref)) {
+    if (j + 1 >= s.mcap) {  // this trajectory's Krylov cap: its basis ends here
+      s.skip = 1;
+      s.msize = s.mcap;
+    } else if (!(bj > B.breakdown_rel * ref)) {
       s.stop = 1;
       s.skip = 1;
       s.msize = j + 1;
@@ -683,7 +690,10 @@ __global__ void __launch_bounds__(kEwThreads) k_b_arn_axpy(BatchDev B, int j, in
     const double beta = sqrt(tot);
     B.hess[((size_t)b * (kBMaxK + 1) + j + 1) * kBMaxK + j] = make_double2(beta, 0.0);
     s.scale = beta > 0.0 ? 1.0 / beta : 0.0;
-    if (j + 1 < B.m) {
+    if (j + 1 >= s.mcap && j + 1 < B.m) {  // this trajectory's Krylov cap: its basis ends here
+      s.skip = 1;
+      s.msize = s.mcap;
+    } else if (j + 1 < B.m) {
       const double2 hd = B.hess[((size_t)b * (kBMaxK + 1) + j) * kBMaxK + j];
       double ref = hypot(hd.x, hd.y);
       if (j > 0) ref += B.hess[((size_t)b * (kBMaxK + 1) + j) * kBMaxK + j - 1].x;
@@ -796,7 +806,10 @@ __global__ void __launch_bounds__(kEwThreads) k_b_reo_axpy(BatchDev B, int j, in
     s.beta[j] = beta;
     s.scale = beta > 0.0 ? 1.0 / beta : 0.0;
     const double ref = fabs(s.alpha[j]) + (j > 0 ? s.beta[j - 1] : 0.0);
-    if (!(beta > B.breakdown_rel * ref)) {
+    if (j + 1 >= s.mcap) {  // this trajectory's Krylov cap: its basis ends here
+      s.skip = 1;
+      s.msize = s.mcap;
+    } else if (!(beta > B.breakdown_rel * ref)) {
       s.stop = 1;
       s.skip = 1;
       s.msize = j + 1;
@@ -1222,6 +1235,7 @@ struct rpm_batch {
   };
   std::vector<ShapeGroup> groups;
   int dot_stride = 1;  // partial-sum slots per trajectory
+  std::vector<int> caps;  // Krylov cap per system (0: the batch's dimension)
 };
 
 namespace rpm {
@@ -1236,7 +1250,7 @@ static void free_graph(rpm_batch* B) {
 
 struct Layout {
   size_t st, V, coef, perr, part, count, gpart, ya, dotpart, dotcount, times, sysof, nof, active, hess, hcur, adots,
-      expm, prog, pcnt, ppart, work, kstatus, total;
+      expm, prog, pcnt, ppart, work, kstatus, capof, total;
 };
 
 static Layout layout(const rpm_batch* B, int ntraj, int ntimes, int nblk, int gblk, int dot_blocks, int ppart_stride,
@@ -1272,6 +1286,7 @@ static Layout layout(const rpm_batch* B, int ntraj, int ntimes, int nblk, int gb
   L.ppart = take(sizeof(double) * (size_t)ntraj * ppart_stride);
   L.work = take(sizeof(unsigned) * (size_t)nwork);
   L.kstatus = take(sizeof(int));
+  L.capof = take(sizeof(int) * ntraj);
   L.total = pos;
   return L;
 }
@@ -1299,6 +1314,7 @@ static HpsiArgs<float2> group_args(const HpsiArgs<float2>& a, int b0, int dstrid
   if (z.stop) z.stop += s * z.istride;
   if (z.skip) z.skip += s * z.istride;
   if (z.msize) z.msize += s * z.istride;
+  if (z.mcap) z.mcap += s * z.istride;
   return c;
 }
 
@@ -1439,6 +1455,7 @@ static void record_step(rpm_batch* Bh, const BatchDev& B, const Layout& L, cudaS
       P.stop = &B.st[G.b0].stop;
       P.skip = &B.st[G.b0].skip;
       P.msize = &B.st[G.b0].msize;
+      P.mcap = &B.st[G.b0].mcap;
       P.istride = kStateInts;
       P.breakdown_rel = B.breakdown_rel;
       P.ya = ya + (size_t)G.b0 * B.ld;
@@ -1480,6 +1497,7 @@ static void record_step(rpm_batch* Bh, const BatchDev& B, const Layout& L, cudaS
     z.stop = &B.st[0].stop;
     z.skip = &B.st[0].skip;
     z.msize = &B.st[0].msize;
+    z.mcap = &B.st[0].mcap;
     z.dstride = kStateDoubles;
     z.istride = kStateInts;
     z.breakdown_rel = B.breakdown_rel;
@@ -1533,9 +1551,11 @@ static void run_batch(rpm_batch* Bh, int ntraj, const int* sys_of, void* psi, co
       fail(RPM_E_INVALID, "Observation times must be nonnegative and strictly increasing.");
   }
   std::vector<long long> n_of(ntraj);
+  std::vector<int> cap_of(ntraj, 0);
   for (int b = 0; b < ntraj; ++b) {
     if (sys_of[b] < 0 || sys_of[b] >= (int)Bh->systems.size()) fail(RPM_E_INVALID, "system index out of range");
     n_of[b] = Bh->systems[sys_of[b]]->n;
+    if (!Bh->caps.empty()) cap_of[b] = Bh->caps[sys_of[b]];
   }
   const int nblk = (int)((Bh->ld + kEwChunk - 1) / kEwChunk);
   const int gblk = std::max(1, std::min(32, (int)((Bh->ld / 4 + kGramChunk - 1) / kGramChunk)));
@@ -1578,6 +1598,8 @@ static void run_batch(rpm_batch* Bh, int ntraj, const int* sys_of, void* psi, co
   check_cuda(cudaMemcpyAsync(base + L.times, times_host, sizeof(double) * ntimes, cudaMemcpyHostToDevice, st), "times");
   check_cuda(cudaMemcpyAsync(base + L.sysof, sys_of, sizeof(int) * ntraj, cudaMemcpyHostToDevice, st), "sys_of");
   check_cuda(cudaMemcpyAsync(base + L.nof, n_of.data(), sizeof(long long) * ntraj, cudaMemcpyHostToDevice, st), "n_of");
+  check_cuda(cudaMemcpyAsync(base + L.capof, cap_of.data(), sizeof(int) * ntraj, cudaMemcpyHostToDevice, st),
+             "cap_of");
   check_cuda(cudaMemcpyAsync(base + L.active, &ntraj, sizeof(int), cudaMemcpyHostToDevice, st), "active");
 
   BatchDev B{};
@@ -1639,7 +1661,7 @@ static void run_batch(rpm_batch* Bh, int ntraj, const int* sys_of, void* psi, co
 
   k_b_setup<<<(ntraj + 127) / 128, 128, 0, st>>>(B, reinterpret_cast<const int*>(base + L.sysof),
                                                  reinterpret_cast<const long long*>(base + L.nof),
-                                                 cfg.initial_step_us);
+                                                 reinterpret_cast<const int*>(base + L.capof), cfg.initial_step_us);
   k_b_init<<<dim3(nblk, ntraj), kEwThreads, 0, st>>>(B);
   check_launch("batched init");
   const size_t ctl_smem = sizeof(double) * 2 * kRecDoubles;
@@ -1697,7 +1719,7 @@ static void run_batch(rpm_batch* Bh, int ntraj, const int* sys_of, void* psi, co
     o.accepted_steps = host[b].steps;
     o.rejected_steps = 0;
     o.matvecs = host[b].matvecs;
-    o.maximum_krylov_dimension = cfg.krylov_dim;
+    o.maximum_krylov_dimension = host[b].mcap;
     o.minimum_step_us = host[b].steps ? host[b].min_step : 0.0;
     o.maximum_step_us = host[b].max_step;
     o.accumulated_state_error = host[b].acc_err;
@@ -1809,6 +1831,21 @@ int rpm_batch_lanczos_kind(const rpm_batch* batch, int* kind) {
   return guarded([&] {
     if (!batch || !kind) fail(RPM_E_INVALID, "bad arguments");
     *kind = batch->persistent ? 0 : batch->fused ? 1 : 2;
+  });
+}
+
+int rpm_batch_set_krylov_caps(rpm_batch* batch, const int* caps, int nsys) {
+  return guarded([&] {
+    if (!batch) fail(RPM_E_INVALID, "batch is NULL");
+    if (nsys == 0 || !caps) {
+      batch->caps.clear();
+      return;
+    }
+    if (nsys != (int)batch->systems.size()) fail(RPM_E_INVALID, "one Krylov cap per system of the batch is required");
+    for (int k = 0; k < nsys; ++k)
+      if (caps[k] != 0 && (caps[k] < 2 || caps[k] > batch->cfg.krylov_dim))
+        fail(RPM_E_INVALID, "Krylov caps must be 0 or in [2, krylov_dim]");
+    batch->caps.assign(caps, caps + nsys);
   });
 }
 

@@ -30,6 +30,8 @@ struct LanczosFuse {
   int* stop;
   int* skip;
   int* msize;
+  const int* mcap;  // Krylov cap of vector b (null: the batch's); the
+                    // iteration j = cap - 1 ends the vector's basis
   int dstride, istride;
   double breakdown_rel;
 };
@@ -92,6 +94,7 @@ struct PersistentLanczos {
   int* stop;
   int* skip;
   int* msize;
+  const int* mcap;  // Krylov cap of vector b at mcap[b * istride]
   int istride;
   double breakdown_rel;
   float2* ya;

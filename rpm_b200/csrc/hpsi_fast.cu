@@ -125,7 +125,11 @@ __device__ void finish_lanczos(const HpsiArgs<float2>& a, int b, double s0, doub
       z.beta_out[(long long)b * z.dstride] = beta;
       z.scale_out[(long long)b * z.dstride] = beta > 0.0 ? 1.0 / beta : 0.0;
       const double ref = fabs(alpha) + (z.first ? 0.0 : z.beta_prev[(long long)b * z.dstride]);
-      if (!(beta > z.breakdown_rel * ref)) {
+      const int cap = z.mcap ? z.mcap[(long long)b * z.istride] : 0x7fffffff;
+      if (z.j + 1 >= cap) {  // this vector's Krylov cap: its basis ends here
+        z.skip[(long long)b * z.istride] = 1;
+        z.msize[(long long)b * z.istride] = cap;
+      } else if (!(beta > z.breakdown_rel * ref)) {
         z.stop[(long long)b * z.istride] = 1;
         z.skip[(long long)b * z.istride] = 1;
         z.msize[(long long)b * z.istride] = z.j + 1;

@@ -463,7 +463,11 @@ __global__ void __maxnreg__(PRegs<CW>::value)
               p.beta[(long long)b * p.dstride + m.j] = beta;
               p.scale[(long long)b * p.dstride] = beta > 0.0 ? 1.0 / beta : 0.0;
               const double ref = fabs(alpha) + (m.j == 0 ? 0.0 : p.beta[(long long)b * p.dstride + m.j - 1]);
-              if (!(beta > p.breakdown_rel * ref)) {
+              const int cap = p.mcap ? p.mcap[(long long)b * p.istride] : p.m;
+              if (m.j + 1 >= cap) {  // this vector's Krylov cap: its basis ends here
+                p.skip[(long long)b * p.istride] = 1;
+                p.msize[(long long)b * p.istride] = cap;
+              } else if (!(beta > p.breakdown_rel * ref)) {
                 p.stop[(long long)b * p.istride] = 1;
                 p.skip[(long long)b * p.istride] = 1;
                 p.msize[(long long)b * p.istride] = m.j + 1;
