@@ -199,6 +199,36 @@ int rpm_singlet_gram(rpm_system* sys, const void* basis_dev, int m, void* gram_d
 int rpm_combine(rpm_system* sys, const void* basis_dev, int m, const void* coef_dev,
                 double scale, void* out_dev, double* norm_host, void* stream);
 
+/* Whole plain propagation of one complex128 state with the singlet
+ * population observable, the reference controller's steps
+ * (ENG:717-933: minimum dimension first, the maximum basis and its ladder
+ * when the minimum misses the step budget, halving on rejection, growth by
+ * 1.5 below a tenth of the budget) decided on the device: per Krylov step
+ * one fixed launch sequence (basis, singlet Gram, candidate spectra and
+ * errors, observation points, new state) and one host read.  The state
+ * (length N, device) is propagated in place to the last completed time;
+ * values_host / state_errors_host (ntimes) receive the populations and the
+ * accumulated state-error estimates at times_host[cursor0 .. points_done).
+ * result->status = 1 when the step fell below minimum_step_us (the caller
+ * raises the reference's error).  Needs maximum_dimension <= 64 and at most
+ * 15 ladder dimensions.  Synchronises `stream`. */
+typedef struct rpm_plain_knobs {
+  int minimum_dimension, maximum_dimension, dimension_increment, embedded_offset;
+  double safety_factor, state_error_budget, initial_step_us, maximum_step_us, minimum_step_us,
+      breakdown_tolerance;
+} rpm_plain_knobs;
+typedef struct rpm_plain_result {
+  int accepted_steps, rejected_steps;
+  long long matvecs;
+  int maximum_krylov_dimension, status;
+  int points_done, pad;
+  double minimum_step_us, maximum_step_us, accumulated_state_error, maximum_norm_error;
+} rpm_plain_result;
+int rpm_plain_propagate(rpm_system* sys, const rpm_plain_knobs* knobs, void* state_dev,
+                        const double* times_host, int ntimes, int cursor0, double norm_error0,
+                        double* values_host, double* state_errors_host, rpm_plain_result* result,
+                        void* stream);
+
 /* Singlet population ||(psi[0,1,:] - psi[1,0,:])/sqrt2||^2 of `batch`
  * complex128 vectors of length n (n divisible by 4, electrons first) spaced
  * `ld` apart (ENG:492-497) into values_host.  Synchronises. */

@@ -67,6 +67,22 @@ class rpm_batch_stats(ctypes.Structure):
                 ("accumulated_state_error", ctypes.c_double), ("maximum_norm_error", ctypes.c_double)]
 
 
+class rpm_plain_knobs(ctypes.Structure):
+    _fields_ = [("minimum_dimension", ctypes.c_int), ("maximum_dimension", ctypes.c_int),
+                ("dimension_increment", ctypes.c_int), ("embedded_offset", ctypes.c_int),
+                ("safety_factor", ctypes.c_double), ("state_error_budget", ctypes.c_double),
+                ("initial_step_us", ctypes.c_double), ("maximum_step_us", ctypes.c_double),
+                ("minimum_step_us", ctypes.c_double), ("breakdown_tolerance", ctypes.c_double)]
+
+
+class rpm_plain_result(ctypes.Structure):
+    _fields_ = [("accepted_steps", ctypes.c_int), ("rejected_steps", ctypes.c_int), ("matvecs", ctypes.c_longlong),
+                ("maximum_krylov_dimension", ctypes.c_int), ("status", ctypes.c_int),
+                ("points_done", ctypes.c_int), ("pad", ctypes.c_int),
+                ("minimum_step_us", ctypes.c_double), ("maximum_step_us", ctypes.c_double),
+                ("accumulated_state_error", ctypes.c_double), ("maximum_norm_error", ctypes.c_double)]
+
+
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _LL = ctypes.c_longlong
@@ -98,6 +114,7 @@ SIGNATURES: dict[str, list] = {
     "rpm_krylov_eval": [_P, _I, ctypes.POINTER(rpm_krylov_req), _D, _D, _P, _I, _P, _I, _PD, _PD, _P],
     "rpm_singlet_gram": [_P, _P, _I, _P, _P],
     "rpm_combine": [_P, _P, _I, _P, _D, _P, _PD, _P],
+    "rpm_plain_propagate": [_P, _P, _P, _PD, _I, _I, _D, _PD, _PD, _P, _P],
     "rpm_singlet_population": [_P, _LL, _I, _LL, _PD, _P],
     "rpm_norm": [_P, _P, _PD, _P],
     "rpm_simpson_yield": [_P, _P, _I, _I, _LL, _D, _P, _P],

@@ -14,8 +14,10 @@
 //     populations (rpm_statevector_engine.py:569-609, 690-715, 521-538).
 //   * Singlet Gram, state recombination, norms and the Simpson yield
 //     (rpm_quantum_needle_jd_sweeps.py:418-420).
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <vector>
 
 #include "common.cuh"
 #include "krylov.cuh"
@@ -382,6 +384,17 @@ __global__ void k_gram_finish(const double2* __restrict__ partials, int nblocks,
   gram[(size_t)k * m + l] = make_double2(0.5 * (s.x + t.x), 0.5 * (s.y - t.y));
 }
 
+static void singlet_gram_launch(rpm_system* sys, const double2* basis, int m, double2* gram, cudaStream_t st) {
+  const long long quarter = sys->n / 4;
+  int blocks = (int)std::min<long long>((quarter + kGramRows - 1) / kGramRows, 2 * 148);
+  blocks = std::max(blocks, 1);
+  auto* partials = static_cast<double2*>(system_scratch(sys, SLOT_GRAM, (size_t)blocks * m * m * sizeof(double2)));
+  const size_t smem = (size_t)kGramRows * m * sizeof(double2);
+  k_gram_partial<<<blocks, kThreads, smem, st>>>(basis, sys->n, m, partials);
+  k_gram_finish<<<(m * m + 255) / 256, 256, 0, st>>>(partials, blocks, m, gram);
+  check_launch("singlet gram");
+}
+
 // ---------------------------------------------------------------------------
 // out = scale * V c  (+ ||out||^2)
 // ---------------------------------------------------------------------------
@@ -517,8 +530,10 @@ static double2* reduce_partials(rpm_system* sys, size_t count) {
 
 static int row_blocks(long long n) { return (int)((n + kRowsPerBlock - 1) / kRowsPerBlock); }
 
-void lanczos_basis(rpm_system* sys, const double2* state, int max_dim, double tol, double2* basis, double* alpha,
-                   double* beta, int* actual, double* norm, cudaStream_t st) {
+// Launches a basis build; the size and ||state|| land in the system's
+// LanczosScalars (stop: 0 full, j + 1 after a breakdown at j, -1 zero vector).
+static void lanczos_basis_launch(rpm_system* sys, const double2* state, int max_dim, double tol, double2* basis,
+                                 double* alpha, double* beta, cudaStream_t st) {
   const long long n = sys->n;
   const int m = (int)std::min<long long>(max_dim, n);
   if (m < 1 || m > RPM_MAX_KRYLOV) fail(RPM_E_UNSUPPORTED, "Krylov dimension must be in [1, 128]");
@@ -541,6 +556,13 @@ void lanczos_basis(rpm_system* sys, const double2* state, int max_dim, double to
     if (j + 1 < m) k_next_vector<<<ew_blocks, 256, 0, st>>>(w, basis + (size_t)(j + 1) * n, n, beta, j, sc);
     check_launch("lanczos step");
   }
+}
+
+void lanczos_basis(rpm_system* sys, const double2* state, int max_dim, double tol, double2* basis, double* alpha,
+                   double* beta, int* actual, double* norm, cudaStream_t st) {
+  const int m = (int)std::min<long long>(max_dim, sys->n);
+  lanczos_basis_launch(sys, state, max_dim, tol, basis, alpha, beta, st);
+  LanczosScalars* sc = scalars(sys);
   struct {
     int stop;
     int pad;
@@ -553,6 +575,421 @@ void lanczos_basis(rpm_system* sys, const double2* state, int max_dim, double to
   *actual = info.stop > 0 ? info.stop : m;
 }
 
+
+// ---------------------------------------------------------------------------
+// Plain propagation with the step controller on the device
+// ---------------------------------------------------------------------------
+// One Krylov step of the reference controller (rpm_statevector_engine.py:
+// 717-933) is a fixed launch sequence with one host read at its end: the
+// basis, the singlet Gram of the basis, k_plain_control (the spectra of every
+// dimension the step's candidate list needs, one warp each; the embedded
+// error of every candidate at the trial step; the first one within the
+// budget; the coefficient row of the new state and the populations and
+// error estimates at the step's observation points), and k_plain_combine
+// (the new state and its norm).  The host only keeps the step-size logic.
+constexpr int kPlainLD = 64;                                  // records for dimensions <= 64
+constexpr int kPlainRec = 2 + kPlainLD + kPlainLD * kPlainLD;  // doubles per spectra record
+constexpr int kPlainWarps = 16;
+constexpr int kPlainMaxCand = 15;                             // candidate dimensions per step
+constexpr int kPlainMaxDims = 2 * kPlainMaxCand + 1;
+
+struct PlainIn {
+  int mode;  // 0: the minimum dimension alone; 1: ladder from the minimum; 2: ladder from minimum + increment
+  int target, built, min_dim, max_dim, inc, offset;
+  int first, npts;  // observation points times[first, first + npts)
+  double trial, budget, safety, t_now;
+};
+
+struct PlainOut {
+  int status;  // 0 accepted, 1 rejected, 2 the maximum basis is needed, 3 eigen-solver failure, 4 zero vector
+  int size, selected, lo, exact, pad;
+  double err, norm, new_norm;
+};
+
+// c_i(t) = sum_k z_ik exp(-i lambda_k t) z_0k for i < m of one record, by one
+// warp into warp-private c (the arithmetic of spectral_coefficients).
+static __device__ void warp_coefficients(const double* rec, double t, double2* ph, double2* c) {
+  const int lane = threadIdx.x & 31;
+  const int m = (int)rec[0];
+  const double* lam = rec + 2;
+  const double* z = rec + 2 + kPlainLD;
+  for (int k = lane; k < m; k += 32) {
+    double s, co;
+    sincos(lam[k] * t, &s, &co);
+    const double w = z[k];
+    ph[k] = make_double2(co * w, -s * w);
+  }
+  __syncwarp();
+  for (int i = lane; i < m; i += 32) {
+    const double* zi = z + i * kPlainLD;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int k = 0; k < m; ++k) {
+      acc.x = fma(zi[k], ph[k].x, acc.x);
+      acc.y = fma(zi[k], ph[k].y, acc.y);
+    }
+    c[i] = acc;
+  }
+  __syncwarp();
+}
+
+// |c_hi - [c_lo; 0]|^2 over the warp.
+static __device__ double warp_diff2(const double2* ch, int mh, const double2* cl, int ml) {
+  double acc = 0.0;
+  for (int i = threadIdx.x & 31; i < mh; i += 32) {
+    double2 d = ch[i];
+    if (i < ml) {
+      d.x -= cl[i].x;
+      d.y -= cl[i].y;
+    }
+    acc = fma(d.x, d.x, fma(d.y, d.y, acc));
+  }
+  return warp_sum(acc);
+}
+
+constexpr size_t kPlainSmem = sizeof(double) * kPlainWarps * 2 * kPlainLD + sizeof(double2) * kPlainWarps * 4 * kPlainLD;
+
+__global__ void __launch_bounds__(kPlainWarps * 32) k_plain_control(const double* __restrict__ alpha,
+                                                                   const double* __restrict__ beta,
+                                                                   const LanczosScalars* sc, PlainIn in, double* recs,
+                                                                   const double2* __restrict__ gram,
+                                                                   const double* __restrict__ times, double* values,
+                                                                   double* perr, double2* coef, PlainOut* out) {
+  extern __shared__ double psm[];
+  __shared__ int s_dims[kPlainMaxDims], s_hi[kPlainMaxCand], s_lo[kPlainMaxCand];
+  __shared__ int s_ndims, s_ncand, s_status, s_sel, s_size, s_exact, s_bad;
+  __shared__ double s_err[kPlainMaxCand], s_norm;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* dd = psm + warp * 2 * kPlainLD;
+  double* ee = dd + kPlainLD;
+  double2* wb = reinterpret_cast<double2*>(psm + kPlainWarps * 2 * kPlainLD) + warp * 4 * kPlainLD;
+  double2* rot = wb;
+  double2* ph = wb + kPlainLD;
+  double2* ch = wb + 2 * kPlainLD;
+  double2* cl = wb + 3 * kPlainLD;
+  if (threadIdx.x == 0) {
+    const int stop = sc->stop;
+    s_norm = sc->norm;
+    s_bad = 0;
+    const int size = stop > 0 ? stop : in.built;
+    const int exact = size < in.target;
+    int nd = 0, nc = 0;
+    auto record = [&](int d) {
+      for (int i = 0; i < nd; ++i)
+        if (s_dims[i] == d) return i;
+      s_dims[nd] = d;
+      return nd++;
+    };
+    // (d, d - offset) as the reference's candidate evaluation (ENG:690-715)
+    auto add = [&](int d) {
+      d = min(d, size);
+      const int lo = max(1, d - in.offset);
+      s_hi[nc] = record(d);
+      s_lo[nc] = lo == d ? -1 : record(lo);
+      ++nc;
+    };
+    if (stop < 0) {
+      nc = 0;
+    } else if (exact) {
+      s_hi[0] = record(size);
+      s_lo[0] = -1;
+      nc = 1;
+    } else if (in.mode == 0) {
+      add(in.min_dim);
+    } else {
+      int last = 0;
+      for (int d = in.mode == 1 ? in.min_dim : in.min_dim + in.inc; d <= in.max_dim; d += in.inc) {
+        add(d);
+        last = d;
+      }
+      if (last != in.max_dim) add(in.max_dim);
+    }
+    s_status = stop < 0 ? 4 : 0;
+    s_size = stop < 0 ? 0 : size;
+    s_exact = exact;
+    s_ndims = nd;
+    s_ncand = nc;
+  }
+  __syncthreads();
+  if (s_status == 0) {
+    for (int r = warp; r < s_ndims; r += kPlainWarps) {
+      const int dim = s_dims[r];
+      double* rec = recs + (size_t)r * kPlainRec;
+      for (int i = lane; i < dim; i += 32) {
+        dd[i] = alpha[i];
+        ee[i] = (i + 1 < dim) ? beta[i] : 0.0;
+      }
+      __syncwarp();
+      const int bad = tridiag_qr_warp<true>(dim, dd, ee, rec + 2 + kPlainLD, kPlainLD, rot);
+      for (int i = lane; i < dim; i += 32) rec[2 + i] = dd[i];
+      if (lane == 0) {
+        rec[0] = dim;
+        rec[1] = bad;
+        if (bad) s_bad = 1;
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+    for (int c = warp; c < s_ncand; c += kPlainWarps) {
+      const double* rh = recs + (size_t)s_hi[c] * kPlainRec;
+      double e2 = 0.0;
+      if (s_lo[c] >= 0) {
+        const double* rl = recs + (size_t)s_lo[c] * kPlainRec;
+        warp_coefficients(rh, in.trial, ph, ch);
+        warp_coefficients(rl, in.trial, ph, cl);
+        e2 = warp_diff2(ch, (int)rh[0], cl, (int)rl[0]);
+      }
+      if (lane == 0) s_err[c] = s_lo[c] >= 0 ? in.safety * s_norm * sqrt(e2) : 0.0;
+      __syncwarp();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int sel = -1;
+      for (int c = 0; c < s_ncand; ++c)
+        if (s_err[c] <= in.budget) {
+          sel = c;
+          break;
+        }
+      s_sel = sel;
+      s_status = s_bad ? 3 : sel >= 0 ? 0 : (in.mode == 0 && in.max_dim > in.min_dim ? 2 : 1);
+    }
+    __syncthreads();
+  }
+  const int status = s_status;
+  if (status == 0) {
+    const int sel = s_sel;
+    const double* rh = recs + (size_t)s_hi[sel] * kPlainRec;
+    const double* rl = s_lo[sel] >= 0 ? recs + (size_t)s_lo[sel] * kPlainRec : nullptr;
+    const int mh = (int)rh[0], ml = rl ? (int)rl[0] : 0;
+    if (warp == 0) {
+      warp_coefficients(rh, in.trial, ph, ch);
+      for (int i = lane; i < mh; i += 32) coef[i] = ch[i];
+    }
+    const double nn = s_norm * s_norm;
+    for (int p = warp; p < in.npts; p += kPlainWarps) {
+      const double dt = times[in.first + p] - in.t_now;
+      warp_coefficients(rh, dt, ph, ch);
+      double e2 = 0.0;
+      if (rl) {
+        warp_coefficients(rl, dt, ph, cl);
+        e2 = warp_diff2(ch, mh, cl, ml);
+      }
+      // c^H G c with the singlet Gram of the basis (leading dimension: the basis size)
+      double v = 0.0;
+      for (int i = lane; i < mh; i += 32) {
+        double2 gc = make_double2(0.0, 0.0);
+        for (int k = 0; k < mh; ++k) gc = cfma(gram[(size_t)i * in.built + k], ch[k], gc);
+        v += ch[i].x * gc.x + ch[i].y * gc.y;
+      }
+      v = warp_sum(v);
+      if (lane == 0) {
+        values[in.first + p] = nn * v;
+        perr[in.first + p] = rl ? in.safety * s_norm * sqrt(e2) : 0.0;
+      }
+      __syncwarp();
+    }
+  }
+  if (threadIdx.x == 0) {
+    PlainOut o{};
+    o.status = status;
+    o.size = s_size;
+    o.exact = s_exact;
+    o.norm = s_norm;
+    if (status == 0) {
+      const int sel = s_sel;
+      o.selected = (int)recs[(size_t)s_hi[sel] * kPlainRec];
+      o.lo = s_lo[sel] >= 0 ? (int)recs[(size_t)s_lo[sel] * kPlainRec] : 0;
+      o.err = s_err[sel];
+    }
+    *out = o;
+  }
+}
+
+// state = ||state|| V c for an accepted step (in place: the basis no longer
+// needs the old state), and ||state|| of the result into out->new_norm.
+__global__ void __launch_bounds__(kThreads) k_plain_combine(const double2* __restrict__ basis, long long n,
+                                                           const double2* __restrict__ coef,
+                                                           double2* __restrict__ state, double2* partials,
+                                                           unsigned* counter, PlainOut* out) {
+  if (out->status != 0) return;
+  __shared__ double2 c[kPlainLD];
+  __shared__ double2 scratch[32];
+  __shared__ double2 tot[1];
+  const int m = out->selected;
+  const double scale = out->norm;
+  for (int k = threadIdx.x; k < m; k += blockDim.x) c[k] = coef[k];
+  __syncthreads();
+  double2 acc[1] = {make_double2(0.0, 0.0)};
+  const long long base = (long long)blockIdx.x * kRowsPerBlock + threadIdx.x;
+#pragma unroll
+  for (int r = 0; r < kRowsPerThread; ++r) {
+    const long long i = base + (long long)r * kThreads;
+    if (i < n) {
+      double2 s = make_double2(0.0, 0.0);
+      for (int k = 0; k < m; ++k) s = cfma(basis[(size_t)k * n + i], c[k], s);
+      s.x *= scale;
+      s.y *= scale;
+      state[i] = s;
+      acc[0].x = fma(s.x, s.x, fma(s.y, s.y, acc[0].x));
+    }
+  }
+  block_sum2<1>(acc, scratch, tot);
+  if (threadIdx.x == 0) partials[blockIdx.x] = tot[0];
+  if (last_block(counter)) {
+    __shared__ double2 res[1];
+    finish_sums(partials, gridDim.x, 1, res);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      out->new_norm = sqrt(res[0].x);
+      *counter = 0;
+    }
+  }
+}
+
+// Device buffers of one plain propagation (stream-ordered allocation).
+struct PlainBuffers {
+  cudaStream_t st = nullptr;
+  void* base = nullptr;
+  double2 *basis = nullptr, *gram = nullptr, *coef = nullptr;
+  double *alpha = nullptr, *beta = nullptr, *recs = nullptr, *times = nullptr, *values = nullptr, *perr = nullptr;
+  PlainOut* out = nullptr;
+  ~PlainBuffers() {
+    if (base) cudaFreeAsync(base, st);
+  }
+};
+
+static void plain_propagate(rpm_system* sys, const rpm_plain_knobs& k, double2* state, const double* times, int ntimes,
+                            int cursor0, double norm_error0, double* values_host, double* errors_host,
+                            rpm_plain_result* res, cudaStream_t st) {
+  const long long n = sys->n;
+  const int mmax = (int)std::min<long long>(k.maximum_dimension, n);
+  PlainBuffers b;
+  b.st = st;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = off;
+    off += (bytes + 255) & ~(size_t)255;
+    return at;
+  };
+  const size_t o_basis = take(sizeof(double2) * (size_t)mmax * n), o_gram = take(sizeof(double2) * 64 * 64),
+               o_coef = take(sizeof(double2) * kPlainLD), o_alpha = take(sizeof(double) * kPlainLD),
+               o_beta = take(sizeof(double) * kPlainLD), o_recs = take(sizeof(double) * kPlainMaxDims * kPlainRec),
+               o_times = take(sizeof(double) * ntimes), o_values = take(sizeof(double) * ntimes),
+               o_perr = take(sizeof(double) * ntimes), o_out = take(sizeof(PlainOut));
+  check_cuda(cudaMallocAsync(&b.base, off, st), "cudaMallocAsync(plain propagation)");
+  char* base = static_cast<char*>(b.base);
+  b.basis = reinterpret_cast<double2*>(base + o_basis);
+  b.gram = reinterpret_cast<double2*>(base + o_gram);
+  b.coef = reinterpret_cast<double2*>(base + o_coef);
+  b.alpha = reinterpret_cast<double*>(base + o_alpha);
+  b.beta = reinterpret_cast<double*>(base + o_beta);
+  b.recs = reinterpret_cast<double*>(base + o_recs);
+  b.times = reinterpret_cast<double*>(base + o_times);
+  b.values = reinterpret_cast<double*>(base + o_values);
+  b.perr = reinterpret_cast<double*>(base + o_perr);
+  b.out = reinterpret_cast<PlainOut*>(base + o_out);
+  // basis slots beyond a breakdown stay finite for the Gram
+  check_cuda(cudaMemsetAsync(b.base, 0, off, st), "cudaMemsetAsync(plain propagation)");
+  check_cuda(cudaMemcpyAsync(b.times, times, sizeof(double) * ntimes, cudaMemcpyHostToDevice, st), "copy times");
+  static bool attr = false;
+  if (!attr) {
+    check_cuda(cudaFuncSetAttribute(k_plain_control, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPlainSmem),
+               "cudaFuncSetAttribute(k_plain_control)");
+    attr = true;
+  }
+  LanczosScalars* sc = scalars(sys);
+  const int nb = row_blocks(n);
+  double2* partials = reduce_partials(sys, (size_t)nb * (RPM_MAX_KRYLOV + 1));
+  PlainOut o{};
+  auto run = [&](const PlainIn& in) {
+    lanczos_basis_launch(sys, state, in.target, k.breakdown_tolerance, b.basis, b.alpha, b.beta, st);
+    if (in.npts > 0) singlet_gram_launch(sys, b.basis, in.built, b.gram, st);
+    k_plain_control<<<1, kPlainWarps * 32, kPlainSmem, st>>>(b.alpha, b.beta, sc, in, b.recs, b.gram, b.times,
+                                                            b.values, b.perr, b.coef, b.out);
+    k_plain_combine<<<nb, kThreads, 0, st>>>(b.basis, n, b.coef, state, partials, &sc->counter[6], b.out);
+    check_launch("plain step");
+    check_cuda(cudaMemcpyAsync(&o, b.out, sizeof(PlainOut), cudaMemcpyDeviceToHost, st), "copy step record");
+    check_cuda(cudaStreamSynchronize(st), "plain step sync");
+  };
+  const double t_end = times[ntimes - 1];
+  double now = 0.0, acc = 0.0, step = t_end > 0.0 ? std::min(k.initial_step_us, t_end) : 0.0;
+  double min_used = 0.0, max_used = 0.0, norm_err = norm_error0;
+  int accepted = 0, rejected = 0, maxdim = 0, cursor = cursor0;
+  long long matvecs = 0;
+  bool prefer_max = false;
+  struct Seg {
+    int first, count;
+    double acc;
+  };
+  std::vector<Seg> segs;
+  res->status = 0;
+  while (cursor < ntimes) {
+    const double trial = std::min(step, t_end - now);
+    if (trial < k.minimum_step_us) {
+      res->status = 1;
+      break;
+    }
+    int c = cursor;
+    while (c < ntimes && times[c] <= now + trial + 1e-13) ++c;
+    PlainIn in{};
+    in.mode = prefer_max ? 1 : 0;
+    in.target = prefer_max ? k.maximum_dimension : k.minimum_dimension;
+    in.built = (int)std::min<long long>(in.target, n);
+    in.min_dim = k.minimum_dimension;
+    in.max_dim = k.maximum_dimension;
+    in.inc = k.dimension_increment;
+    in.offset = k.embedded_offset;
+    in.first = cursor;
+    in.npts = c - cursor;
+    in.trial = trial;
+    in.budget = k.state_error_budget * trial / std::max(t_end, trial);
+    in.safety = k.safety_factor;
+    in.t_now = now;
+    run(in);
+    matvecs += o.size;
+    if (o.status == 2) {  // the minimum dimension missed the budget: the maximum basis, ladder from min + increment
+      prefer_max = true;
+      in.mode = 2;
+      in.target = k.maximum_dimension;
+      in.built = mmax;
+      run(in);
+      matvecs += o.size;
+    }
+    if (o.status == 4) fail(RPM_E_INVALID, "Cannot propagate the zero vector.");
+    if (o.status == 3) fail(RPM_E_NUMERIC, "tridiagonal eigen-solver did not converge");
+    if (o.status == 1) {
+      ++rejected;
+      step = 0.5 * trial;
+      continue;
+    }
+    maxdim = std::max(maxdim, o.selected);
+    if (o.selected > k.minimum_dimension) prefer_max = true;
+    if (c > cursor) segs.push_back({cursor, c - cursor, acc});
+    cursor = c;
+    now = now + trial;
+    acc += o.err;
+    min_used = accepted ? std::min(min_used, trial) : trial;
+    max_used = accepted ? std::max(max_used, trial) : trial;
+    ++accepted;
+    norm_err = std::max(norm_err, std::fabs(o.new_norm - 1.0));
+    step = o.err < 0.1 * in.budget ? std::min(k.maximum_step_us, 1.5 * trial) : trial;
+  }
+  std::vector<double> perr(ntimes);
+  check_cuda(cudaMemcpyAsync(values_host + cursor0, b.values + cursor0, sizeof(double) * (ntimes - cursor0),
+                             cudaMemcpyDeviceToHost, st), "copy values");
+  check_cuda(cudaMemcpyAsync(perr.data(), b.perr, sizeof(double) * ntimes, cudaMemcpyDeviceToHost, st), "copy errors");
+  check_cuda(cudaStreamSynchronize(st), "plain propagation sync");
+  for (const Seg& s : segs)
+    for (int i = s.first; i < s.first + s.count; ++i) errors_host[i] = s.acc + perr[i];
+  res->accepted_steps = accepted;
+  res->rejected_steps = rejected;
+  res->matvecs = matvecs;
+  res->maximum_krylov_dimension = maxdim;
+  res->minimum_step_us = min_used;
+  res->maximum_step_us = max_used;
+  res->accumulated_state_error = acc;
+  res->maximum_norm_error = norm_err;
+  res->points_done = cursor;
+}
 }  // namespace rpm
 
 using namespace rpm;
@@ -625,15 +1062,39 @@ int rpm_singlet_gram(rpm_system* sys, const void* basis_dev, int m, void* gram_d
     if (m < 1 || m > 64) fail(RPM_E_UNSUPPORTED, "Gram size must be in [1, 64]");
     if (sys->ndims < 2 || sys->dims[0] != 2 || sys->dims[1] != 2)
       fail(RPM_E_INVALID, "The first two axes must be the two electron spins.");
-    auto st = static_cast<cudaStream_t>(stream);
-    const long long quarter = sys->n / 4;
-    int blocks = (int)std::min<long long>((quarter + kGramRows - 1) / kGramRows, 2 * 148);
-    blocks = std::max(blocks, 1);
-    auto* partials = static_cast<double2*>(system_scratch(sys, SLOT_GRAM, (size_t)blocks * m * m * sizeof(double2)));
-    const size_t smem = (size_t)kGramRows * m * sizeof(double2);
-    k_gram_partial<<<blocks, kThreads, smem, st>>>(static_cast<const double2*>(basis_dev), sys->n, m, partials);
-    k_gram_finish<<<(m * m + 255) / 256, 256, 0, st>>>(partials, blocks, m, static_cast<double2*>(gram_dev));
-    check_launch("singlet gram");
+    singlet_gram_launch(sys, static_cast<const double2*>(basis_dev), m, static_cast<double2*>(gram_dev),
+                        static_cast<cudaStream_t>(stream));
+  });
+}
+
+int rpm_plain_propagate(rpm_system* sys, const rpm_plain_knobs* knobs, void* state_dev, const double* times_host,
+                        int ntimes, int cursor0, double norm_error0, double* values_host, double* state_errors_host,
+                        rpm_plain_result* result, void* stream) {
+  return guarded([&] {
+    if (!sys || !knobs || !state_dev || !times_host || !values_host || !state_errors_host || !result)
+      fail(RPM_E_INVALID, "NULL argument");
+    if (!sys->on_device) fail(RPM_E_INVALID, "system was created host-only");
+    if (sys->non_hermitian)
+      fail(RPM_E_UNSUPPORTED, "Lanczos needs a Hermitian Hamiltonian; unequal recombination rates run on the "
+                              "batched propagator (Arnoldi)");
+    if (sys->ndims < 2 || sys->dims[0] != 2 || sys->dims[1] != 2)
+      fail(RPM_E_INVALID, "The first two axes must be the two electron spins.");
+    const rpm_plain_knobs& k = *knobs;
+    if (k.minimum_dimension <= k.embedded_offset || k.embedded_offset < 0)
+      fail(RPM_E_INVALID, "minimum_dimension must exceed embedded_offset.");
+    if (k.maximum_dimension < k.minimum_dimension)
+      fail(RPM_E_INVALID, "maximum_dimension must not be smaller than minimum_dimension.");
+    if (k.maximum_dimension > kPlainLD) fail(RPM_E_UNSUPPORTED, "device-driven steps support Krylov dimension <= 64");
+    if (k.dimension_increment < 1) fail(RPM_E_INVALID, "dimension_increment must be positive");
+    if ((k.maximum_dimension - k.minimum_dimension) / k.dimension_increment + 2 > kPlainMaxCand)
+      fail(RPM_E_UNSUPPORTED, "device-driven steps support at most 15 candidate dimensions");
+    if (ntimes < 1 || cursor0 < 0 || cursor0 > ntimes) fail(RPM_E_INVALID, "bad observation range");
+    for (int i = 0; i < ntimes; ++i)
+      if (!(times_host[i] >= 0.0) || (i && !(times_host[i] > times_host[i - 1])))
+        fail(RPM_E_INVALID, "Observation times must be nonnegative and strictly increasing.");
+    *result = rpm_plain_result{};
+    plain_propagate(sys, k, static_cast<double2*>(state_dev), times_host, ntimes, cursor0, norm_error0, values_host,
+                    state_errors_host, result, static_cast<cudaStream_t>(stream));
   });
 }
 

@@ -482,7 +482,8 @@ class AdaptiveLanczosPropagator:
     def __init__(self, hamiltonian, *, minimum_dimension: int = 24, maximum_dimension: int = 64,
                  dimension_increment: int = 8, embedded_offset: int = 4, safety_factor: float = 2.0,
                  state_error_budget: float = 2.4e-5, initial_step_us: float = 0.05, maximum_step_us: float = 0.25,
-                 minimum_step_us: float = 1e-9, breakdown_tolerance: float = 1e-14) -> None:
+                 minimum_step_us: float = 1e-9, breakdown_tolerance: float = 1e-14,
+                 device_steps: bool = True) -> None:
         if minimum_dimension <= embedded_offset:
             raise ValueError("minimum_dimension must exceed embedded_offset.")
         if maximum_dimension < minimum_dimension:
@@ -500,6 +501,9 @@ class AdaptiveLanczosPropagator:
         self.maximum_step_us = maximum_step_us
         self.minimum_step_us = minimum_step_us
         self.breakdown_tolerance = breakdown_tolerance
+        # device_steps: with the singlet observable, decide every step on the
+        # device (rpm_plain_propagate); False keeps the host-driven loop
+        self.device_steps = device_steps
         self._buffers_for = None
 
     # -- device buffers ---------------------------------------------------------
@@ -569,6 +573,35 @@ class AdaptiveLanczosPropagator:
                   _lib.ptr(coef_row), float(scale), _lib.ptr(out), ctypes.byref(norm), _lib.stream_handle())
         return norm.value
 
+    def _native_steps(self) -> bool:
+        """Whether the whole step loop can run as device-driven steps (rpm_plain_propagate)."""
+        return (self.device_steps and self.maximum_dimension <= 64 and self.dimension_increment >= 1 and self.embedded_offset >= 0
+                and (self.maximum_dimension - self.minimum_dimension) // self.dimension_increment + 2 <= 15)
+
+    def _propagate_native(self, state, times, cursor, values, bounds, state_errors, norm_error0):
+        """The reference's step loop (ENG:717-933) with every decision taken on the
+        device; one host read per Krylov step (singlet population observable)."""
+        knobs = _lib.rpm_plain_knobs(self.minimum_dimension, self.maximum_dimension, self.dimension_increment,
+                                     self.embedded_offset, self.safety_factor, self.state_error_budget,
+                                     self.initial_step_us, self.maximum_step_us, self.minimum_step_us,
+                                     self.breakdown_tolerance)
+        res = _lib.rpm_plain_result()
+        t = np.ascontiguousarray(times, dtype=np.float64)
+        _lib.call("rpm_plain_propagate", self.hamiltonian._system.handle, ctypes.byref(knobs), _lib.ptr(state),
+                  _lib.dptr(t), int(t.size), int(cursor), float(norm_error0), _lib.dptr(values),
+                  _lib.dptr(state_errors), ctypes.byref(res), _lib.stream_handle())
+        self.hamiltonian.matvec_count += int(res.matvecs)
+        if res.status == 1:
+            raise RuntimeError("Lanczos step fell below the configured minimum.")
+        for at in range(cursor, t.size):
+            bounds[at] = state_error_to_population_bound(state_errors[at])
+        stats = PropagationStats(
+            accepted_steps=res.accepted_steps, rejected_steps=res.rejected_steps, matvecs=int(res.matvecs),
+            maximum_krylov_dimension=res.maximum_krylov_dimension, minimum_step_us=res.minimum_step_us,
+            maximum_step_us=res.maximum_step_us, accumulated_state_error=res.accumulated_state_error,
+            maximum_norm_error=res.maximum_norm_error)
+        return PropagationResult(times, values, bounds, state_errors, None, state.cpu().numpy(), stats)
+
     def _ladder(self, start):
         dims = list(range(start, self.maximum_dimension + 1, self.dimension_increment))
         if not dims or dims[-1] != self.maximum_dimension:
@@ -626,6 +659,8 @@ class AdaptiveLanczosPropagator:
             if stored is not None:
                 stored[0] = state.cpu().numpy()
             cursor = 1
+        if gpu_singlet and progress_callback is None and self._native_steps():
+            return self._propagate_native(state, times, cursor, values, bounds, state_errors, maximum_norm_error)
         final_time = float(times[-1])
         step = min(self.initial_step_us, final_time) if final_time else 0.0
         prefer_max = False
