@@ -713,7 +713,7 @@ def main() -> None:
                    help="run the step's trajectories as this many concurrent batches on their own streams")
     p.add_argument("--reserve-sms", type=int, default=16,
                    help="with --parts > 1: SMs each persistent launch leaves to the other batch's kernels")
-    p.add_argument("--persistent-warps", type=int, choices=(8, 10), default=8,
+    p.add_argument("--persistent-warps", type=int, choices=(8, 9, 10), default=8,
                    help="persistent kernel: consumer warps per CTA")
     p.add_argument("--reorth-period", type=int, default=0,
                    help="reorthogonalise the next Lanczos vector every this many iterations (0: never)")

@@ -337,8 +337,9 @@ int rpm_batch_counters(rpm_batch* batch, int reset, long long* kernel_launches, 
  * (per segment between reorthogonalisations), 1 shape-specialised pass pairs
  * per iteration, 2 general cube kernels (or Arnoldi). */
 int rpm_batch_lanczos_kind(const rpm_batch* batch, int* kind);
-/* Consumer warps per CTA of the persistent Lanczos kernel, 8 or 10 (default
- * 8); a tuning knob for measurements, no counterpart in the reference. */
+/* Consumer warps per CTA of the persistent Lanczos kernel, 8, 9 or 10
+ * (default 8); a tuning knob for measurements, no counterpart in the
+ * reference. */
 int rpm_set_persistent_warps(int consumer_warps);
 /* Per-system Krylov dimensions (caps[k] for the batch's system k, 0: the
  * batch's krylov_dim; otherwise 2 <= cap <= krylov_dim): a trajectory's

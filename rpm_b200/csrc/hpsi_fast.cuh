@@ -324,12 +324,16 @@ __device__ __forceinline__ void r_tile_math(const T* tab, const ORec<T>* orec, c
 // the pass-R partial y_vec and writes out_vec (when `store`).  `pair` is the
 // 4 x 4 electron-pair operator, HR the right radical's half size.
 // Accumulates sf <x, out>, |out|^2 and |x|^2 over its elements (x: the staged
-// input).
+// input).  `pbuf` (complex64 only; nullptr: direct loads): this warp's
+// 2 KiB shared-memory buffer, into which each task's pass-R partial is copied
+// by 16-byte cp.async (L2 only) when the task starts and read back when it
+// ends, so the copy's latency overlaps the task's arithmetic without holding
+// registers.  Buffer layout: segment ((e 4 + i) 4 + h 2 + lg) of 8 columns.
 template <class T, int N1, int NH>
 __device__ __forceinline__ void l_tile_math(const T* tab, const ORec<T>* orec, const T* tile, const T* pair, int HR,
                                             int c0, long long quarter, const T* y_vec, T* out_vec,
                                             typename FastT<T>::R sf, bool store, int warp, int nwarps, double& dot,
-                                            double& nw, double& nv) {
+                                            double& nw, double& nv, T* pbuf = nullptr) {
   using P = PassL<T, N1, NH>;
   using S = typename P::S;
   using R = typename FastT<T>::R;
@@ -375,10 +379,28 @@ __device__ __forceinline__ void l_tile_math(const T* tab, const ORec<T>* orec, c
     const ORec<T> rec = orec[o];
     const int lo = o * 8 + lg * 4;  // l of cube element i = 0
     T pb[2][4];  // pass-R partial of the cube (with -beta_{j-1} v_{j-1} when fused), loaded early
+    bool staged = false;
+    if constexpr (P::EPU == 2) {
+      if (pbuf) {
+        // 32 segments of 8 consecutive columns (64 bytes), four 16-byte copies each
 #pragma unroll
-    for (int e = 0; e < 2; ++e)
+        for (int k = 0; k < 4; ++k) {
+          const int cidx = lane + 32 * k;
+          const int seg = cidx >> 2, piece = cidx & 3;
+          const int se = seg >> 4, si = (seg >> 2) & 3, sh = (seg >> 1) & 1, sg = seg & 1;
+          copy16(pbuf + seg * 8 + 2 * piece,
+                 y_vec + (2 * se + sh) * quarter + (long long)(o * 8 + sg * 4 + si) * HR + c0 + 2 * piece);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        staged = true;
+      }
+    }
+    if (!staged) {
 #pragma unroll
-      for (int i = 0; i < 4; ++i) pb[e][i] = __ldcg(y_b + 2 * e * quarter + (long long)(lo + i) * HR);
+      for (int e = 0; e < 2; ++e)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) pb[e][i] = __ldcg(y_b + 2 * e * quarter + (long long)(lo + i) * HR);
+    }
     T x[2][4], acc[2][4];
 #pragma unroll
     for (int e = 0; e < 2; ++e)
@@ -413,6 +435,17 @@ __device__ __forceinline__ void l_tile_math(const T* tab, const ORec<T>* orec, c
         outer_coefs<S>(tab, k, m, mp, cc);
         partner((mp - m) * S::gs(k), c, cc);
       }
+    }
+    if (staged) {
+      // every lane's copies have landed before any lane reads the buffer, and
+      // every lane has read it before the next task's copies overwrite it
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+      __syncwarp();
+#pragma unroll
+      for (int e = 0; e < 2; ++e)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) pb[e][i] = pbuf[((e * 4 + i) * 4 + h * 2 + lg) * 8 + j];
+      __syncwarp();
     }
     R part = 0, pw = 0, px = 0;
 #pragma unroll

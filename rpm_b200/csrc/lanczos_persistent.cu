@@ -169,7 +169,11 @@ struct PShape {
       align128c(cmax((PR::NO * 24 + 15) / 16 * 16, (PL::NO * 24 + 15) / 16 * 16 + 128));
   static constexpr int R_TILE_BYTES = TR * PR::RS * 8;  // one padded R tile
   static constexpr int L_TILE_BYTES = 2 * HL * 16 * 8;
-  static constexpr int TILE_BYTES = align128c(cmax(2 * R_TILE_BYTES, L_TILE_BYTES));
+  // an L stage also holds one 2 KiB pass-R partial buffer per consumer warp
+  static constexpr int kMaxConsumerWarps = 10;
+  static constexpr int PBUF_BYTES = 2048;
+  static constexpr int TILE_BYTES =
+      align128c(cmax(2 * R_TILE_BYTES, L_TILE_BYTES + kMaxConsumerWarps * PBUF_BYTES));
   static constexpr int STAGE = TAB_BYTES + OREC_BYTES + TILE_BYTES;
   static constexpr int SMEM = 2 * STAGE + 1024;  // + alignment slack
 };
@@ -252,6 +256,7 @@ __global__ void __maxnreg__(PRegs<CW>::value)
   constexpr int OREC_R = ((PR::NO * 24) + 15) / 16 * 16;
   constexpr int OREC_L = ((PL::NO * 24) + 15) / 16 * 16 + 128;  // + the pair operator
   static_assert(OREC_R <= PS::OREC_BYTES && OREC_L <= PS::OREC_BYTES, "outer records exceed their stage slot");
+  static_assert(CW <= PS::kMaxConsumerWarps, "an L stage holds the partial buffers of at most kMaxConsumerWarps warps");
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
@@ -550,8 +555,9 @@ __global__ void __maxnreg__(PRegs<CW>::value)
       } else {
         const float2* pair = reinterpret_cast<const float2*>(reinterpret_cast<const char*>(orec) + OREC_L - 128);
         double dot = 0.0, nw = 0.0, nv = 0.0;
+        float2* pbuf = tile + PS::L_TILE_BYTES / 8 + warp * (PS::PBUF_BYTES / 8);
         l_tile_math<float2, N1L, NHL>(tab, orec, tile, pair, HR, m.tile * 8, QUARTER, yb, vj + p.ld, 1.0f,
-                                      m.j < p.m - 1, warp, CW, dot, nw, nv);
+                                      m.j < p.m - 1, warp, CW, dot, nw, nv, pbuf);
         dot = warp_sum_d(dot);
         nw = warp_sum_d(nw);
         nv = warp_sum_d(nv);
@@ -642,15 +648,16 @@ void launch_instance(const PersistentLanczos& p, const float2* V_base, long long
 
 using Launcher = void (*)(const PersistentLanczos&, const float2*, long long, cudaStream_t);
 
-// Consumer warps per CTA (8 or 10; set by rpm_set_persistent_warps): with the
-// producer and finisher warps both keep 168 registers per thread; 8 splits
+// Consumer warps per CTA (8, 9 or 10; set by rpm_set_persistent_warps): with
+// the producer and finisher warps all keep 168 registers per thread; 8 splits
 // the full system's 24 pass-R warp tasks evenly (the combine barrier waits
-// for the slowest warp), 10 hides more latency.
+// for the slowest warp), 9 its 36 pass-L tasks, 10 hides more latency.
 std::atomic<int> g_consumer_warps{8};
 
 template <int N1L, int NHL, int N1R, int NHR>
 Launcher by_warps(int warps) {
   switch (warps) {
+    case 9: return launch_instance<N1L, NHL, N1R, NHR, 9>;
     case 10: return launch_instance<N1L, NHL, N1R, NHR, 10>;
     default: return launch_instance<N1L, NHL, N1R, NHR, 8>;
   }
@@ -696,7 +703,7 @@ bool launch_lanczos_persistent(const PersistentLanczos& p, const CubePlan& plan,
 
 extern "C" int rpm_set_persistent_warps(int consumer_warps) {
   return rpm::guarded([&] {
-    if (consumer_warps != 8 && consumer_warps != 10) rpm::fail(RPM_E_INVALID, "consumer warps must be 8 or 10");
+    if (consumer_warps < 8 || consumer_warps > 10) rpm::fail(RPM_E_INVALID, "consumer warps must be 8, 9 or 10");
     rpm::g_consumer_warps.store(consumer_warps, std::memory_order_relaxed);
   });
 }

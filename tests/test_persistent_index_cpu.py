@@ -46,7 +46,9 @@ class PShape:
         self.OREC_BYTES = align128(max(self.OREC_R, self.OREC_L))
         self.R_TILE = self.TR * self.RS * 8
         self.L_TILE = 2 * self.HL * 16 * 8
-        self.TILE_BYTES = align128(max(2 * self.R_TILE, self.L_TILE))
+        self.PBUF = 2048  # one pass-R partial buffer per consumer warp, after the L tile
+        self.MAX_CW = 10
+        self.TILE_BYTES = align128(max(2 * self.R_TILE, self.L_TILE + self.MAX_CW * self.PBUF))
         self.STAGE = self.TAB_BYTES + self.OREC_BYTES + self.TILE_BYTES
         self.SMEM = 2 * self.STAGE + 1024
         self.Q = self.HL * self.HR
@@ -148,3 +150,40 @@ def test_stage_layout_and_copy_addresses(shape):
                 assert dst % 128 == 0 and dst + ps.BL * 16 * 8 <= ps.L_TILE <= ps.TILE_BYTES
     part_stride = 3 * ps.LT
     assert (47 * part_stride + (ps.LT - 1) * 3 + 2) < 48 * part_stride
+
+
+@pytest.mark.parametrize("shape", sorted(SHAPES))
+def test_pass_l_partial_staging_matches_direct_loads(shape):
+    """The per-warp cp.async staging of the pass-R partial (l_tile_math with a
+    buffer): every 16-byte copy reads inside the vector from a 16-byte aligned
+    address and lands inside the warp's 2 KiB buffer, the copies cover the
+    buffer exactly once, and every lane reads back exactly the element the
+    direct loads would have read."""
+    ps = PShape(*SHAPES[shape])
+    no = ps.HL // 8
+    for cw in (8, 9, 10):
+        assert ps.L_TILE + cw * ps.PBUF <= ps.TILE_BYTES
+    for tile in range(ps.LT):
+        c0 = tile * 8
+        for o in range(no):
+            buf = {}
+            for lane in range(32):
+                for k in range(4):
+                    cidx = lane + 32 * k
+                    seg, piece = divmod(cidx, 4)
+                    se, si, sh, sg = seg >> 4, (seg >> 2) & 3, (seg >> 1) & 1, seg & 1
+                    src = (2 * se + sh) * ps.Q + (o * 8 + sg * 4 + si) * ps.HR + c0 + 2 * piece
+                    dst = seg * 8 + 2 * piece
+                    assert src % 2 == 0 and 0 <= src and src + 2 <= ps.N
+                    assert 0 <= dst and dst + 2 <= ps.PBUF // 8
+                    for u in range(2):
+                        assert dst + u not in buf
+                        buf[dst + u] = src + u
+            assert len(buf) == ps.PBUF // 8
+            for lane in range(32):
+                j, h, lg = lane & 7, (lane >> 3) & 1, lane >> 4
+                lo = o * 8 + lg * 4
+                for e in (0, 1):
+                    for i in range(4):
+                        direct = h * ps.Q + c0 + j + 2 * e * ps.Q + (lo + i) * ps.HR
+                        assert buf[((e * 4 + i) * 4 + h * 2 + lg) * 8 + j] == direct
