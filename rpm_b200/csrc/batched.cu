@@ -284,7 +284,8 @@ __global__ void __launch_bounds__(kEwThreads) k_b_update(BatchDev B, int j, int 
 // One warp: c = exp(-i T_hi t) e1 (into `c` when non-null) and the embedded
 // error safety * norm * |c_hi(t) - [c_lo(t); 0]| (0 when `exact`), the
 // reference's estimate (rpm_statevector_engine.py:690-715).  ph: 2 * kBMaxK
-// warp-private scratch.  Records follow the krylov.cuh layout (LD = kBMaxK).
+// warp-private scratch.  Records: [0] size, [1] status, [2, 2 + kBMaxK)
+// eigenvalues, then the eigenvectors by columns (tridiag_qr_warp_cols, ld kBMaxK).
 __device__ double warp_step_error(const double* rec_hi, const double* rec_lo, bool exact, double t, double safety,
                                   double norm, double2* ph, double2* c) {
   const int lane = threadIdx.x & 31;
@@ -298,7 +299,7 @@ __device__ double warp_step_error(const double* rec_hi, const double* rec_lo, bo
     const int kk = hi ? k : k - mh;
     double sv, cv;
     sincos((hi ? lh : ll)[kk] * t, &sv, &cv);
-    const double w = (hi ? zh : zl)[kk];
+    const double w = (hi ? zh : zl)[kk * kBMaxK];  // first component of eigenvector kk
     ph[k] = make_double2(cv * w, -sv * w);
   }
   __syncwarp();
@@ -306,14 +307,14 @@ __device__ double warp_step_error(const double* rec_hi, const double* rec_lo, bo
   for (int i = lane; i < mh; i += 32) {
     double2 ch = make_double2(0.0, 0.0), cl = make_double2(0.0, 0.0);
     for (int k = 0; k < mh; ++k) {
-      const double zz = zh[i * kBMaxK + k];
+      const double zz = zh[k * kBMaxK + i];
       ch.x = fma(zz, ph[k].x, ch.x);
       ch.y = fma(zz, ph[k].y, ch.y);
     }
     if (c) c[i] = ch;
     if (i < ml) {
       for (int k = 0; k < ml; ++k) {
-        const double zz = zl[i * kBMaxK + k];
+        const double zz = zl[k * kBMaxK + i];
         cl.x = fma(zz, ph[mh + k].x, cl.x);
         cl.y = fma(zz, ph[mh + k].y, cl.y);
       }
@@ -358,7 +359,7 @@ __global__ void __launch_bounds__(128) k_b_control(BatchDev B) {
       ee[warp][i] = (i + 1 < dim) ? s.beta[i] : 0.0;
     }
     __syncwarp();
-    const int bad = tridiag_qr_warp<false>(dim, dd[warp], ee[warp], rec + 2 + kBMaxK, kBMaxK, rot[warp]);
+    const int bad = tridiag_qr_warp_cols(dim, dd[warp], ee[warp], rec + 2 + kBMaxK, kBMaxK, rot[warp]);
     for (int i = lane; i < dim; i += 32) rec[2 + i] = dd[warp][i];
     if (lane == 0) {
       rec[0] = dim;

@@ -235,6 +235,96 @@ static __device__ int tridiag_qr_warp(int m, double* d, double* e, double* z, in
   }
 }
 
+// The same decomposition, faster: every lane tests its off-diagonal entries
+// for deflation and the active block [p, q] comes from two ballots; lane 0
+// computes the shift and chases the bulge, carrying the entries the next
+// rotation reads in registers (the operations and their order are those of
+// the textbook sweep); every lane applies the sweep's rotations to its rows
+// of the eigenvector matrix.  Rotations are normalised with rsqrt.  d, e:
+// diagonal and off-diagonal (d -> eigenvalues); m <= 64.  z: m x m
+// eigenvector matrix stored by columns, z[k * ldz + i] = component i of
+// eigenvector k, so that the lanes' row updates touch consecutive addresses.
+// Returns 0 on convergence.
+static __device__ int tridiag_qr_warp_cols(int m, double* d, double* e, double* z, int ldz, double2* rot) {
+  const int lane = threadIdx.x & 31;
+  for (int idx = lane; idx < m * m; idx += 32) {
+    const int k = idx / m, i = idx - k * m;
+    z[k * ldz + i] = (i == k) ? 1.0 : 0.0;
+  }
+  __syncwarp();
+  int sweeps = 0;
+  while (true) {
+    // deflation: e[i] negligible against its neighbours on the diagonal
+    bool nz[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int i = lane + 32 * h;
+      nz[h] = false;
+      if (i + 1 < m) {
+        const double ei = e[i];
+        if (fabs(ei) <= DBL_EPSILON * (fabs(d[i]) + fabs(d[i + 1])) || fabs(ei) < DBL_MIN) e[i] = 0.0;
+        else nz[h] = true;
+      }
+    }
+    const unsigned long long nzm = (unsigned long long)__ballot_sync(0xffffffffu, nz[0]) |
+                                   ((unsigned long long)__ballot_sync(0xffffffffu, nz[1]) << 32);
+    __syncwarp();
+    // q - 1: the last nonzero off-diagonal; p: the start of its unreduced block
+    const int q = nzm ? 64 - __clzll(nzm) : 0;
+    if (q == 0) return 0;
+    if (++sweeps > 40 * m) return 1;
+    const unsigned long long below = q >= 2 ? (~nzm) & ((1ull << (q - 1)) - 1ull) : 0ull;
+    const int p = below ? 64 - __clzll(below) : 0;
+    if (lane == 0) {
+      const double delta = 0.5 * (d[q - 1] - d[q]);
+      const double eq = e[q - 1];
+      const double denom = delta + copysign(hypot(delta, eq), delta);
+      const double mu = d[q] - eq * eq / denom;
+      double x = d[p] - mu, y = e[p];
+      double a = d[p], bb = e[p];  // d[k] and e[k] as the previous rotation left them
+      for (int k = p; k < q; ++k) {
+        const double cc = d[k + 1];
+        const double en = k + 1 < q ? e[k + 1] : 0.0;
+        double c = 1.0, sn = 0.0, r = 0.0;
+        const double rr = fma(x, x, y * y);
+        if (rr > 0.0) {
+          const double inv = rsqrt(rr);
+          c = x * inv;
+          sn = y * inv;
+          r = rr * inv;
+        }
+        if (k > p) e[k - 1] = r;
+        const double dk = c * c * a + 2.0 * c * sn * bb + sn * sn * cc;
+        const double dk1 = sn * sn * a - 2.0 * c * sn * bb + c * c * cc;
+        const double ek = c * sn * (cc - a) + (c * c - sn * sn) * bb;
+        d[k] = dk;
+        d[k + 1] = dk1;
+        e[k] = ek;
+        if (k + 1 < q) {
+          x = ek;
+          y = sn * en;
+          bb = c * en;
+          e[k + 1] = bb;
+        }
+        a = dk1;
+        rot[k] = make_double2(c, sn);
+      }
+    }
+    __syncwarp();
+    for (int i = lane; i < m; i += 32) {
+      double zk = z[p * ldz + i];
+      for (int k = p; k < q; ++k) {
+        const double2 cs = rot[k];
+        const double zk1 = z[(k + 1) * ldz + i];
+        z[k * ldz + i] = cs.x * zk + cs.y * zk1;
+        zk = -cs.y * zk + cs.x * zk1;
+      }
+      z[q * ldz + i] = zk;
+    }
+    __syncwarp();
+  }
+}
+
 // c = exp(-i T t) e1 from a spectra record, into shared `c` (m entries).
 // Record layout with leading dimension LD: [0] size, [1] status, [2, 2+LD)
 // eigenvalues, then LD x LD eigenvectors (row i = component i).
