@@ -916,15 +916,33 @@ __global__ void __launch_bounds__(kEwThreads) k_b_rebuild(BatchDev B) {
   const float2* V = B.V + (size_t)b * (B.m + 1) * B.ld;
   double2* x = B.psi + (size_t)b * B.ld;
   double nn = 0.0;
+  // the thread's kEwPer elements are summed side by side (independent loads
+  // and accumulation chains per basis vector); each element's sum runs over
+  // k in ascending order
+  const long long i0 = (long long)blockIdx.x * kEwChunk + threadIdx.x;
   const long long end = min(s.n, (long long)(blockIdx.x + 1) * kEwChunk);
-  for (long long i = (long long)blockIdx.x * kEwChunk + threadIdx.x; i < end; i += kEwThreads) {
-    double2 acc = make_double2(0.0, 0.0);
-    for (int k = 0; k < M; ++k) {
-      const float2 v = V[(size_t)k * B.ld + i];
-      acc = cfma(cc[k], make_double2(v.x, v.y), acc);
+  double2 acc[kEwPer];
+#pragma unroll
+  for (int e = 0; e < kEwPer; ++e) acc[e] = make_double2(0.0, 0.0);
+  for (int k = 0; k < M; ++k) {
+    const float2* vk = V + (size_t)k * B.ld;
+    const double2 ck = cc[k];
+    float2 v[kEwPer];
+#pragma unroll
+    for (int e = 0; e < kEwPer; ++e) {
+      const long long i = i0 + (long long)e * kEwThreads;
+      v[e] = i < end ? vk[i] : make_float2(0.f, 0.f);
     }
-    x[i] = acc;
-    nn = fma(acc.x, acc.x, fma(acc.y, acc.y, nn));
+#pragma unroll
+    for (int e = 0; e < kEwPer; ++e) acc[e] = cfma(ck, make_double2(v[e].x, v[e].y), acc[e]);
+  }
+#pragma unroll
+  for (int e = 0; e < kEwPer; ++e) {
+    const long long i = i0 + (long long)e * kEwThreads;
+    if (i < end) {
+      x[i] = acc[e];
+      nn = fma(acc[e].x, acc[e].x, fma(acc[e].y, acc[e].y, nn));
+    }
   }
   nn = block_sum(nn, red);
   if (threadIdx.x == 0) B.part[((size_t)b * B.nblk + blockIdx.x) * 2] = nn;
