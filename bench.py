@@ -484,6 +484,7 @@ def b200_arm(args, rank: int, world: int, dist) -> None:
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     torch.cuda.set_device(dev)
     _lib.call("rpm_set_persistent_warps", args.persistent_warps)
+    _lib.call("rpm_set_gram_kernel", 1 if args.gram == "tensor" else 0)
     full = synthetic.full_system()
     dirs = synthetic.fibonacci_sphere(args.orientations)
     hams = [rb.CompiledFullPairHamiltonian(full.dimensions, full.terms(th, ph), left_axes=full.left_axes,
@@ -713,6 +714,8 @@ def main() -> None:
                    help="run the step's trajectories as this many concurrent batches on their own streams")
     p.add_argument("--reserve-sms", type=int, default=16,
                    help="with --parts > 1: SMs each persistent launch leaves to the other batch's kernels")
+    p.add_argument("--gram", choices=("tensor", "cuda"), default="tensor",
+                   help="singlet Gram kernel: tcgen05 tensor cores or CUDA cores")
     p.add_argument("--persistent-warps", type=int, choices=(8, 9, 10), default=8,
                    help="persistent kernel: consumer warps per CTA")
     p.add_argument("--reorth-period", type=int, default=0,

@@ -337,6 +337,13 @@ int rpm_batch_counters(rpm_batch* batch, int reset, long long* kernel_launches, 
  * (per segment between reorthogonalisations), 1 shape-specialised pass pairs
  * per iteration, 2 general cube kernels (or Arnoldi). */
 int rpm_batch_lanczos_kind(const rpm_batch* batch, int* kind);
+/* Kernel of the batched singlet Gram V^H P_S V (replaces the per-basis
+ * projection of ENG:521-529): 0 the CUDA-core kernel, 1 (default) the
+ * tensor-core kernel (tcgen05, TF32 split into high and low parts, FP32 sums
+ * over 128 rows in tensor memory, FP64 across them) wherever the batch allows
+ * it (every state dimension a multiple of 8, Krylov dimension <= 63).  Read
+ * when a batch's step is set up. */
+int rpm_set_gram_kernel(int kernel);
 /* Consumer warps per CTA of the persistent Lanczos kernel, 8, 9 or 10
  * (default 8); a tuning knob for measurements, no counterpart in the
  * reference. */

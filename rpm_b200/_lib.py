@@ -126,6 +126,7 @@ SIGNATURES: dict[str, list] = {
     "rpm_batch_lanczos_kind": [_P, _PI],
     "rpm_batch_set_krylov_caps": [_P, _PI, _I],
     "rpm_set_persistent_warps": [_I],
+    "rpm_set_gram_kernel": [_I],
     "rpm_batch_counters": [_P, _I, _PLL, _PLL, _PD, _PLL],
     "rpm_adjoint_create": [_I, _LL, _LL, _I, _I, _I, ctypes.POINTER(_P)],
     "rpm_adjoint_destroy": [_P],

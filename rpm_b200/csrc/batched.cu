@@ -22,6 +22,7 @@
 // err(dt) <= budget * dt / T is taken.  Because the basis does not depend on
 // dt, no step is ever rejected.
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
 #include <cmath>
 #include <memory>
@@ -1132,6 +1133,8 @@ __global__ void __launch_bounds__(256) k_b_observe(BatchDev B) {
 // ---------------------------------------------------------------------------
 }  // namespace rpm
 
+#include "gram_tc.cuh"
+
 struct rpm_batch {
   std::vector<rpm_system*> systems;
   rpm_batch_config cfg{};
@@ -1167,6 +1170,7 @@ struct rpm_batch {
   int probe_iters = 1;      // Lanczos iterations between the probe events
   bool fused = false;       // every group runs the fused passes
   bool persistent = false;  // every group runs the persistent Lanczos kernel
+  bool gram_tc = false;     // the singlet Gram runs on the tensor cores (k_b_gram_tc)
   // Consecutive trajectories whose systems share one shape (digit pattern and
   // layout) form a group; each group's H psi is one launch pair with its own
   // plan, on the shape-specialised passes when the shape allows.
@@ -1181,6 +1185,21 @@ struct rpm_batch {
 };
 
 namespace rpm {
+
+// Which kernel forms the singlet Gram (rpm_set_gram_kernel): 0 the CUDA-core
+// k_b_gram, 1 the tensor-core k_b_gram_tc where the batch allows it.
+static std::atomic<int> g_gram_kernel{1};
+
+// The singlet Gram of the step's basis, on the side stream (it overlaps the
+// controller and the rebuild).
+static void launch_gram(const rpm_batch* Bh, const BatchDev& B) {
+  if (Bh->gram_tc) {
+    const CUtensorMap map = basis_rows_map(B.V, (long long)B.ntraj * (B.m + 1), B.ld, gramtc::kGC, B.m + 1);
+    gramtc::k_b_gram_tc<<<dim3(B.gblk, B.ntraj), gramtc::kThreads, gramtc::kSmemBytes, Bh->side>>>(map, B);
+  }
+  else
+    k_b_gram<<<dim3(B.gblk, B.ntraj), 256, 0, Bh->side>>>(B);
+}
 
 static void free_graph(rpm_batch* B) {
   if (B->exec) cudaGraphExecDestroy(B->exec);
@@ -1335,7 +1354,7 @@ static void record_step(rpm_batch* Bh, const BatchDev& B, const Layout& L, cudaS
     Bh->launches_per_step = 1 + (per_iter + 4) * m + 4;
     check_cuda(cudaEventRecord(Bh->ev_fork, st), "fork record");
     check_cuda(cudaStreamWaitEvent(Bh->side, Bh->ev_fork, 0), "fork wait");
-    k_b_gram<<<dim3(B.gblk, B.ntraj), 256, 0, Bh->side>>>(B);
+    launch_gram(Bh, B);
     check_cuda(cudaEventRecord(Bh->ev_join, Bh->side), "join record");
     k_b_control_arn<<<B.ntraj, 128, kArnCtlSmem, st>>>(B);
     k_b_rebuild<<<ew, kEwThreads, 0, st>>>(B);
@@ -1472,7 +1491,7 @@ static void record_step(rpm_batch* Bh, const BatchDev& B, const Layout& L, cudaS
   const size_t ctl_smem = sizeof(double) * 2 * kRecDoubles;
   check_cuda(cudaEventRecord(Bh->ev_fork, st), "fork record");
   check_cuda(cudaStreamWaitEvent(Bh->side, Bh->ev_fork, 0), "fork wait");
-  k_b_gram<<<dim3(B.gblk, B.ntraj), 256, 0, Bh->side>>>(B);
+  launch_gram(Bh, B);
   check_cuda(cudaEventRecord(Bh->ev_join, Bh->side), "join record");
   k_b_control<<<B.ntraj, 128, ctl_smem, st>>>(B);
   k_b_rebuild<<<ew, kEwThreads, 0, st>>>(B);
@@ -1501,6 +1520,10 @@ static void run_batch(rpm_batch* Bh, int ntraj, const int* sys_of, void* psi, co
   }
   const int nblk = (int)((Bh->ld + kEwChunk - 1) / kEwChunk);
   const int gblk = std::max(1, std::min(32, (int)((Bh->ld / 4 + kGramChunk - 1) / kGramChunk)));
+  // tensor-core Gram: 16-byte aligned bulk copies need n / 4 even, and the
+  // basis (m + 1 vectors) fits the 64 rows per real part of its operand
+  Bh->gram_tc = g_gram_kernel.load(std::memory_order_relaxed) == 1 && cfg.krylov_dim + 1 <= gramtc::kMaxBasis;
+  for (int b = 0; b < ntraj && Bh->gram_tc; ++b) Bh->gram_tc = n_of[b] % 8 == 0;
   // shape groups: runs of consecutive trajectories whose systems share a shape
   Bh->groups.clear();
   for (int b = 0; b < ntraj;) {
@@ -1609,6 +1632,10 @@ static void run_batch(rpm_batch* Bh, int ntraj, const int* sys_of, void* psi, co
   const size_t ctl_smem = sizeof(double) * 2 * kRecDoubles;
   check_cuda(cudaFuncSetAttribute(k_b_control, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctl_smem),
              "control attr");
+  if (Bh->gram_tc)
+    check_cuda(cudaFuncSetAttribute(gramtc::k_b_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    gramtc::kSmemBytes),
+               "tensor-core Gram attr");
   check_cuda(cudaFuncSetAttribute(k_b_observe, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(sizeof(double2) * kBMaxK * kBMaxK)),
              "observe attr");
@@ -1638,7 +1665,7 @@ static void run_batch(rpm_batch* Bh, int ntraj, const int* sys_of, void* psi, co
     check_cuda(cudaMemcpyAsync(&active, base + L.active, sizeof(int), cudaMemcpyDeviceToHost, st), "poll");
     check_cuda(cudaMemcpyAsync(&kstatus, base + L.kstatus, sizeof(int), cudaMemcpyDeviceToHost, st), "poll");
     check_cuda(cudaStreamSynchronize(st), "poll sync");
-    if (kstatus) fail(RPM_E_TIMEOUT, "persistent Lanczos kernel: a device wait gave up (time limit)");
+    if (kstatus) fail(RPM_E_TIMEOUT, "persistent Lanczos or tensor-core Gram kernel: a device wait gave up (time limit)");
     if (active == ntraj) {
       float ms = 0.f;
       if (cudaEventElapsedTime(&ms, Bh->probe0, Bh->probe1) == cudaSuccess) {
@@ -1693,6 +1720,13 @@ static void release_batch(rpm_batch* batch) {
 using namespace rpm;
 
 extern "C" {
+
+int rpm_set_gram_kernel(int kernel) {
+  return rpm::guarded([&] {
+    if (kernel != 0 && kernel != 1) rpm::fail(RPM_E_INVALID, "Gram kernel must be 0 (CUDA cores) or 1 (tensor cores)");
+    rpm::g_gram_kernel.store(kernel, std::memory_order_relaxed);
+  });
+}
 
 int rpm_batch_create(rpm_system* const* systems, int nsys, const rpm_batch_config* cfg, rpm_batch** out) {
   return guarded([&] {

@@ -1,6 +1,8 @@
 // Launch interface of the H psi kernels (hpsi.cu), shared with batched.cu.
 #pragma once
 
+#include <cuda.h>
+
 #include "common.cuh"
 
 namespace rpm {
@@ -116,6 +118,9 @@ bool launch_lanczos_persistent(const PersistentLanczos& p, const CubePlan& plan,
 // L tiles per vector and iteration of the persistent kernel for a shape (8
 // columns per electron-B half each), 0 when the shape has no instance.
 int persistent_l_tiles(const CubePlan& plan);
+// 2-D tensor map of a basis buffer [nslots][ld] complex64: a box of box_rows
+// consecutive elements of box_slots consecutive slots lands as [slot][box_rows].
+CUtensorMap basis_rows_map(const float2* V, long long nslots, long long ld, int box_rows, int box_slots);
 
 int sm_count();
 // Same dimensions, digit pattern and layout (offset tables) of the two radicals.

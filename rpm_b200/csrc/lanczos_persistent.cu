@@ -40,13 +40,14 @@
 #include "common.cuh"
 #include "hpsi.cuh"
 #include "hpsi_fast.cuh"
+#include "ptx.cuh"
 
 namespace rpm {
 namespace {
 
 using namespace fastpass;
+using namespace ptx;
 
-constexpr long long kWaitCycles = 4000000000LL;  // about 2 s at 1.965 GHz
 constexpr int kTabCache = 256;                   // vectors whose table pointers are cached in shared memory
 
 constexpr int align128c(int b) { return (b + 127) & ~127; }
@@ -59,49 +60,8 @@ __device__ __forceinline__ double warp_sum_d(double v) {
 }
 
 // ---------------------------------------------------------------------------
-// PTX helpers: mbarrier, bulk / tensor copies, acquire / release
+// PTX helpers: tensor copies, acquire / release (mbarriers and bulk copies: ptx.cuh)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_test(unsigned long long* bar, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Wait for phase `parity` of `bar` to complete; false after the time limit
-// or when another thread already raised the status word.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, int* status) {
-  const long long t0 = clock64();
-  for (int spin = 0;; ++spin) {
-    if (mbar_test(bar, parity)) return true;
-    if ((spin & 63) == 63) {
-      if (*reinterpret_cast<volatile int*>(status)) return false;
-      if (clock64() - t0 > kWaitCycles) {
-        atomicExch(status, 1);
-        return false;
-      }
-    }
-  }
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
-}
 __device__ __forceinline__ void tma_5d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3, int c4,
                                        unsigned long long* bar) {
   asm volatile(
@@ -679,6 +639,26 @@ Launcher pick(const CubePlan& plan, int* ltiles) {
 }
 
 }  // namespace
+
+// 2-D map of a basis buffer [nslots][ld] complex64 (elements as 8-byte words)
+// with a box of box_rows consecutive elements of box_slots consecutive slots;
+// one tensor copy lands as [slot][box_rows].
+CUtensorMap basis_rows_map(const float2* V, long long nslots, long long ld, int box_rows, int box_slots) {
+  CUtensorMap map;
+  if (nslots < 1 || nslots > 0x7fffffffLL || box_rows < 1 || box_rows > 256 || box_slots < 1 || box_slots > 256 ||
+      (box_rows * 8) % 16 != 0 || (ld * 8) % 16 != 0 || (reinterpret_cast<uintptr_t>(V) & 15u))
+    fail(RPM_E_UNSUPPORTED, "basis rows map: unsupported sizes or alignment");
+  cuuint64_t dims[2] = {(cuuint64_t)ld, (cuuint64_t)nslots};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * 8};
+  cuuint32_t box[2] = {(cuuint32_t)box_rows, (cuuint32_t)box_slots};
+  cuuint32_t estr[2] = {1, 1};
+  const CUresult r = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, const_cast<float2*>(V), dims, strides, box,
+                                 estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    fail(RPM_E_CUDA, "cuTensorMapEncodeTiled failed for the basis rows map (" + std::to_string((int)r) + ")");
+  return map;
+}
 
 int persistent_l_tiles(const CubePlan& plan) {
   int lt = 0;
