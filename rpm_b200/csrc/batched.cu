@@ -360,7 +360,7 @@ __global__ void __launch_bounds__(128) k_b_control(BatchDev B) {
       ee[warp][i] = (i + 1 < dim) ? s.beta[i] : 0.0;
     }
     __syncwarp();
-    const int bad = tridiag_qr_warp_cols(dim, dd[warp], ee[warp], rec + 2 + kBMaxK, kBMaxK, rot[warp]);
+    const int bad = tridiag_qr_warp_cols<true>(dim, dd[warp], ee[warp], rec + 2 + kBMaxK, kBMaxK, rot[warp]);
     for (int i = lane; i < dim; i += 32) rec[2 + i] = dd[warp][i];
     if (lane == 0) {
       rec[0] = dim;

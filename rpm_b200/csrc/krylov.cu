@@ -587,7 +587,8 @@ void lanczos_basis(rpm_system* sys, const double2* state, int max_dim, double to
 // budget; the coefficient row of the new state and the populations and
 // error estimates at the step's observation points), and k_plain_combine
 // (the new state and its norm).  The host only keeps the step-size logic.
-constexpr int kPlainLD = 64;                                  // records for dimensions <= 64
+// records for dimensions <= 64: [0] size, [1] status, eigenvalues, eigenvectors by columns
+constexpr int kPlainLD = 64;
 constexpr int kPlainRec = 2 + kPlainLD + kPlainLD * kPlainLD;  // doubles per spectra record
 constexpr int kPlainWarps = 16;
 constexpr int kPlainMaxCand = 15;                             // candidate dimensions per step
@@ -616,16 +617,16 @@ static __device__ void warp_coefficients(const double* rec, double t, double2* p
   for (int k = lane; k < m; k += 32) {
     double s, co;
     sincos(lam[k] * t, &s, &co);
-    const double w = z[k];
+    const double w = z[k * kPlainLD];  // first component of eigenvector k
     ph[k] = make_double2(co * w, -s * w);
   }
   __syncwarp();
   for (int i = lane; i < m; i += 32) {
-    const double* zi = z + i * kPlainLD;
     double2 acc = make_double2(0.0, 0.0);
     for (int k = 0; k < m; ++k) {
-      acc.x = fma(zi[k], ph[k].x, acc.x);
-      acc.y = fma(zi[k], ph[k].y, acc.y);
+      const double zz = z[k * kPlainLD + i];
+      acc.x = fma(zz, ph[k].x, acc.x);
+      acc.y = fma(zz, ph[k].y, acc.y);
     }
     c[i] = acc;
   }
@@ -719,7 +720,7 @@ __global__ void __launch_bounds__(kPlainWarps * 32) k_plain_control(const double
         ee[i] = (i + 1 < dim) ? beta[i] : 0.0;
       }
       __syncwarp();
-      const int bad = tridiag_qr_warp<true>(dim, dd, ee, rec + 2 + kPlainLD, kPlainLD, rot);
+      const int bad = tridiag_qr_warp_cols<false>(dim, dd, ee, rec + 2 + kPlainLD, kPlainLD, rot);
       for (int i = lane; i < dim; i += 32) rec[2 + i] = dd[i];
       if (lane == 0) {
         rec[0] = dim;

@@ -149,102 +149,19 @@ static __device__ int tridiag_qr(int m, double* d, double* e, double* z, int ldz
 // Tridiagonal eigen-decomposition by one warp
 // ---------------------------------------------------------------------------
 // Implicit symmetric tridiagonal QR with Wilkinson shifts (Golub & Van Loan,
-// section 8.3) run by ONE warp: lane 0 deflates and chases the bulge, every
-// lane applies the sweep's rotations to its rows of the eigenvector matrix.
-// HYPOT = false normalises the rotations with rsqrt instead of hypot and two
-// divisions (magnitudes here are far from the overflow range); HYPOT = true
-// matches the block-wide solver's arithmetic.  d, e: diagonal and
-// off-diagonal (d -> eigenvalues); z: m x m, row i = component i, leading
-// dimension ldz.  Returns 0 on convergence.
-template <bool HYPOT>
-static __device__ int tridiag_qr_warp(int m, double* d, double* e, double* z, int ldz, double2* rot) {
-  const int lane = threadIdx.x & 31;
-  for (int idx = lane; idx < m * m; idx += 32) {
-    const int i = idx / m, k = idx - i * m;
-    z[i * ldz + k] = (i == k) ? 1.0 : 0.0;
-  }
-  __syncwarp();
-  int sweeps = 0;
-  while (true) {
-    int p = 0, q = 0, state = 0;
-    if (lane == 0) {
-      for (int i = 0; i + 1 < m; ++i)
-        if (fabs(e[i]) <= DBL_EPSILON * (fabs(d[i]) + fabs(d[i + 1])) || fabs(e[i]) < DBL_MIN) e[i] = 0.0;
-      q = m - 1;
-      while (q > 0 && e[q - 1] == 0.0) --q;
-      if (q == 0) {
-        state = 1;
-      } else if (++sweeps > 40 * m) {
-        state = 2;
-      } else {
-        p = q - 1;
-        while (p > 0 && e[p - 1] != 0.0) --p;
-        const double delta = 0.5 * (d[q - 1] - d[q]);
-        const double eq = e[q - 1];
-        const double denom = delta + copysign(hypot(delta, eq), delta);
-        const double mu = d[q] - eq * eq / denom;
-        double x = d[p] - mu, y = e[p];
-        for (int k = p; k < q; ++k) {
-          double c = 1.0, sn = 0.0, r = 0.0;
-          if (HYPOT) {
-            r = hypot(x, y);
-            if (r > 0.0) {
-              c = x / r;
-              sn = y / r;
-            }
-          } else {
-            const double rr = fma(x, x, y * y);
-            if (rr > 0.0) {
-              const double inv = rsqrt(rr);
-              c = x * inv;
-              sn = y * inv;
-              r = rr * inv;
-            }
-          }
-          if (k > p) e[k - 1] = r;
-          const double a = d[k], bb = e[k], cc = d[k + 1];
-          d[k] = c * c * a + 2.0 * c * sn * bb + sn * sn * cc;
-          d[k + 1] = sn * sn * a - 2.0 * c * sn * bb + c * c * cc;
-          e[k] = c * sn * (cc - a) + (c * c - sn * sn) * bb;
-          if (k + 1 < q) {
-            x = e[k];
-            y = sn * e[k + 1];
-            e[k + 1] = c * e[k + 1];
-          }
-          rot[k] = make_double2(c, sn);
-        }
-      }
-    }
-    state = __shfl_sync(0xffffffffu, state, 0);
-    p = __shfl_sync(0xffffffffu, p, 0);
-    q = __shfl_sync(0xffffffffu, q, 0);
-    __syncwarp();
-    if (state != 0) return state == 1 ? 0 : 1;
-    for (int i = lane; i < m; i += 32) {
-      double* row = z + i * ldz;
-      double zk = row[p];
-      for (int k = p; k < q; ++k) {
-        const double2 cs = rot[k];
-        const double zk1 = row[k + 1];
-        row[k] = cs.x * zk + cs.y * zk1;
-        zk = -cs.y * zk + cs.x * zk1;
-      }
-      row[q] = zk;
-    }
-    __syncwarp();
-  }
-}
-
-// The same decomposition, faster: every lane tests its off-diagonal entries
+// section 8.3) run by ONE warp: every lane tests its off-diagonal entries
 // for deflation and the active block [p, q] comes from two ballots; lane 0
-// computes the shift and chases the bulge, carrying the entries the next
-// rotation reads in registers (the operations and their order are those of
-// the textbook sweep); every lane applies the sweep's rotations to its rows
-// of the eigenvector matrix.  Rotations are normalised with rsqrt.  d, e:
-// diagonal and off-diagonal (d -> eigenvalues); m <= 64.  z: m x m
-// eigenvector matrix stored by columns, z[k * ldz + i] = component i of
-// eigenvector k, so that the lanes' row updates touch consecutive addresses.
-// Returns 0 on convergence.
+// computes the shift and chases the bulge; every lane applies the sweep's
+// rotations to its rows of the eigenvector matrix.  d, e: diagonal and
+// off-diagonal (d -> eigenvalues); m <= 64.  z: m x m eigenvector matrix
+// stored by columns, z[k * ldz + i] = component i of eigenvector k, so that
+// the lanes' row updates touch consecutive addresses.  FAST = true normalises
+// the rotations with rsqrt and carries the entries the next rotation reads in
+// registers; FAST = false keeps the block-wide solver's arithmetic exactly
+// (hypot and two divisions, operands re-read from memory), so that the plain
+// path's decisions stay those matched to the reference.  Returns 0 on
+// convergence.
+template <bool FAST>
 static __device__ int tridiag_qr_warp_cols(int m, double* d, double* e, double* z, int ldz, double2* rot) {
   const int lane = threadIdx.x & 31;
   for (int idx = lane; idx < m * m; idx += 32) {
@@ -275,7 +192,33 @@ static __device__ int tridiag_qr_warp_cols(int m, double* d, double* e, double* 
     if (++sweeps > 40 * m) return 1;
     const unsigned long long below = q >= 2 ? (~nzm) & ((1ull << (q - 1)) - 1ull) : 0ull;
     const int p = below ? 64 - __clzll(below) : 0;
-    if (lane == 0) {
+    if (lane == 0 && !FAST) {
+      const double delta = 0.5 * (d[q - 1] - d[q]);
+      const double eq = e[q - 1];
+      const double denom = delta + copysign(hypot(delta, eq), delta);
+      const double mu = d[q] - eq * eq / denom;
+      double x = d[p] - mu, y = e[p];
+      for (int k = p; k < q; ++k) {
+        double c = 1.0, sn = 0.0;
+        const double r = hypot(x, y);
+        if (r > 0.0) {
+          c = x / r;
+          sn = y / r;
+        }
+        if (k > p) e[k - 1] = r;
+        const double a = d[k], bb = e[k], cc = d[k + 1];
+        d[k] = c * c * a + 2.0 * c * sn * bb + sn * sn * cc;
+        d[k + 1] = sn * sn * a - 2.0 * c * sn * bb + c * c * cc;
+        e[k] = c * sn * (cc - a) + (c * c - sn * sn) * bb;
+        if (k + 1 < q) {
+          x = e[k];
+          y = sn * e[k + 1];
+          e[k + 1] = c * e[k + 1];
+        }
+        rot[k] = make_double2(c, sn);
+      }
+    }
+    if (lane == 0 && FAST) {
       const double delta = 0.5 * (d[q - 1] - d[q]);
       const double eq = e[q - 1];
       const double denom = delta + copysign(hypot(delta, eq), delta);
