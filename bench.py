@@ -671,7 +671,7 @@ def b200_arm(args, rank: int, world: int, dist) -> None:
                                                       "random-phase vectors per GPU per step",
                        "trajectories_per_step_per_gpu": per_rank, "krylov_dim": krylov, "tile": tile,
                        "concurrent_parts": args.parts,
-                       "reorth_period": reorth, "lanczos_kernel": kind,
+                       "reorth_period": reorth, "lanczos_kernel": kind, "gram_kernel": args.gram,
                        "tuning": ("autotuned: Krylov " + str(list(KRYLOV_RANGE)) + ", tile, reorthogonalisation "
                                   "(none / 16), accuracy-gated" if tuning else "fixed"),
                        "state_error_budget": budget, "parallelism": f"replicas x{world} (cost-balanced shards)",

@@ -28,6 +28,14 @@ def test_library_exports_every_declared_symbol():
     assert lib.rpm_version() >= 1
 
 
+def test_measurement_knobs_reject_unknown_values():
+    # host-side setters: no device work, so they run on a machine without a GPU
+    for name, bad, good in (("rpm_set_gram_kernel", 2, 1), ("rpm_set_persistent_warps", 7, 8)):
+        with pytest.raises(ValueError, match="must be"):  # RPM_E_INVALID maps to ValueError
+            _lib.call(name, bad)
+        _lib.call(name, good)
+
+
 def test_device_count_without_gpu_is_a_clean_zero_or_more():
     assert _lib.device_count() >= 0
 
