@@ -337,6 +337,26 @@ int rpm_batch_counters(rpm_batch* batch, int reset, long long* kernel_launches, 
  * (per segment between reorthogonalisations), 1 shape-specialised pass pairs
  * per iteration, 2 general cube kernels (or Arnoldi). */
 int rpm_batch_lanczos_kind(const rpm_batch* batch, int* kind);
+/* Factorized exact oracle (rpm_quantum_needle_reproduction.py:127-240):
+ * batched Hermitian eigen-decomposition of n x n complex matrices (replaces
+ * the per-radical numpy.linalg.eigh of diagonalize_radical, :127): a_dev
+ * holds `batch` row-major matrices (overwritten), w_dev receives the
+ * eigenvalues in ascending order (batch x n), v_dev the eigenvectors as
+ * columns (v[i * n + j] = component i of eigenvector j); Householder
+ * tridiagonalisation, implicit tridiagonal QR, back-transformation, all FP64.
+ * work_dev: rpm_he_eigh_workspace bytes.  Synchronises the stream. */
+int rpm_he_eigh_workspace(int n, int batch, long long* bytes);
+int rpm_he_eigh(int n, int batch, void* a_dev, double* w_dev, void* v_dev, void* work_dev, cudaStream_t stream);
+/* C = A^H B for `batch` square complex128 matrices (row-major): the
+ * eigenbasis spin operators of diagonalize_radical (:127-170). */
+int rpm_zgemm_hn(int n, int batch, const void* a_dev, const void* b_dev, void* c_dev, cudaStream_t stream);
+/* Radix-2 complex128 FFT of `batch` rows of power-of-two length n in place
+ * (scratch: n x batch complex); inverse = 1 gives the unscaled inverse
+ * transform.  With rpm_spectrum_mac (acc += x * y element-wise) it forms the
+ * convolution of binned transition spectra (convolved_correlation_spectrum,
+ * :175-201). */
+int rpm_fft_pow2(int n, int batch, void* data_dev, void* scratch_dev, int inverse, cudaStream_t stream);
+int rpm_spectrum_mac(long long count, void* acc_dev, const void* x_dev, const void* y_dev, cudaStream_t stream);
 /* Kernel of the batched singlet Gram V^H P_S V (replaces the per-basis
  * projection of ENG:521-529): 0 the CUDA-core kernel, 1 (default) the
  * tensor-core kernel (tcgen05, TF32 split into high and low parts, FP32 sums

@@ -105,6 +105,11 @@ SIGNATURES: dict[str, list] = {
     "rpm_system_fast_hpsi": [_P, _PI],
     "rpm_reduced_density": [_P, _LL, _LL, _P, _I, _P, _LL, _P, _P],
     "rpm_bin_transition_lines": [_P, _P, _P, _I, _D, _D, _LL, _P, _P, _P],
+    "rpm_he_eigh_workspace": [_I, _I, _P],
+    "rpm_he_eigh": [_I, _I, _P, _P, _P, _P, _P],
+    "rpm_zgemm_hn": [_I, _I, _P, _P, _P, _P],
+    "rpm_fft_pow2": [_I, _I, _P, _P, _I, _P],
+    "rpm_spectrum_mac": [_LL, _P, _P, _P, _P],
     "rpm_schmidt_norms": [_P, _LL, _LL, _P, _I, _P, _LL, _P, _P, _P],
     "rpm_system_set_recombination": [_P, _D, _D],
     "rpm_system_recombination": [_P, _PD, _PD, _PI],

@@ -3,8 +3,9 @@
 Every observable here is a function of the reduced density matrix of one
 side of a bipartition, rho_A = M M^H with M the state reshaped to
 (kept part) x (traced part).  rho_A is formed on the GPU by the library's
-``rpm_reduced_density`` kernels (FP64) and diagonalised by the GPU batched
-Hermitian eigen-solver (at most the smaller side's dimension); the Schmidt
+``rpm_reduced_density`` kernels (FP64) and diagonalised by the library's
+batched FP64 Hermitian eigen-solver (``rpm_he_eigh``; at most the smaller
+side's dimension); the Schmidt
 coefficients are then the row norms of U^H M (``rpm_schmidt_norms``), which
 resolves small coefficients to ~eps |M| where square roots of rho_A's
 eigenvalues would only resolve ~sqrt(eps).  States may be one vector or a batch
@@ -31,6 +32,7 @@ import numpy as np
 
 from . import _lib
 from .engine import _torch
+from .factorized import hermitian_eigh
 
 
 def _offsets(dimensions: Sequence[int], axes: Sequence[int]) -> np.ndarray:
@@ -92,7 +94,7 @@ def pure_log_negativity(state, dimensions: Sequence[int], left_axes: Sequence[in
     rest = tuple(a for a in range(len(dims)) if a not in kept)
     x, single = _as_batch(state, math.prod(dims))
     rho = reduced_density(x, dims, kept)
-    _, vec = torch.linalg.eigh(rho)
+    _, vec = hermitian_eigh(rho)  # the library's FP64 eigen-solver
     vec = vec.contiguous()
     # Schmidt norms |U^H M| row by row (accurate for small Schmidt values)
     offa = torch.from_numpy(_offsets(dims, kept)).to("cuda")
@@ -144,7 +146,7 @@ def mixed_two_electron_log_negativity_batch(rho) -> np.ndarray:
     m = torch.from_numpy(np.ascontiguousarray(matrices.reshape(-1, 4, 4))).to("cuda")
     herm = 0.5 * (m + m.conj().transpose(-1, -2))
     partial = herm.reshape(-1, 2, 2, 2, 2).permute(0, 3, 2, 1, 4).reshape(-1, 4, 4)
-    lam = torch.linalg.eigvalsh(partial)
+    lam, _ = hermitian_eigh(partial.contiguous())
     values = torch.clamp(torch.log2(lam.abs().sum(dim=-1)), min=0.0)
     return values.cpu().numpy().reshape(leading)
 
