@@ -26,7 +26,7 @@ from typing import Sequence
 import numpy as np
 
 from . import _lib
-from .engine import MatrixFreeHamiltonian, PropagationStats, _torch, state_error_to_population_bound
+from .engine import MatrixFreeHamiltonian, PropagationStats, _torch, population_bounds
 
 
 @dataclass(frozen=True)
@@ -258,7 +258,7 @@ class BatchedPropagator:
             yields = self.yields_device(times, values, lifetime_us).cpu().numpy()
         vals = values.cpu().numpy()
         se = errs.cpu().numpy()
-        bounds = np.vectorize(state_error_to_population_bound)(se) if se.size else se
+        bounds = population_bounds(se) if se.size else se
         status = np.array([s.status for s in stats], dtype=np.int32)
         st = tuple(PropagationStats(s.accepted_steps, s.rejected_steps, int(s.matvecs), s.maximum_krylov_dimension,
                                     s.minimum_step_us, s.maximum_step_us, s.accumulated_state_error,
@@ -377,7 +377,7 @@ def propagate_segments_batched(initial_states, times_us, segments: Sequence[Batc
         _lib.call("rpm_simpson_yield", _lib.ptr(t), _lib.ptr(vt), int(times.size), ntraj, int(times.size),
                   float(lifetime_us), _lib.ptr(out), _lib.stream_handle())
         yields = out.cpu().numpy()
-    bounds = np.vectorize(state_error_to_population_bound)(errors)
+    bounds = population_bounds(errors)
     st = tuple(PropagationStats(int(accepted[b]), 0, int(matvecs[b]), int(krylov_dimension),
                                 float(min_step[b]) if np.isfinite(min_step[b]) else 0.0, float(max_step[b]),
                                 float(accumulated[b]), 0.0) for b in range(ntraj))

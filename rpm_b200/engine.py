@@ -423,6 +423,14 @@ def state_error_to_population_bound(state_error: float) -> float:
     return min(1.0, 2.0 * epsilon + epsilon * epsilon)
 
 
+def population_bounds(state_errors) -> np.ndarray:
+    """state_error_to_population_bound over an array, element by element with
+    the same operations (negative errors and NaN count as zero)."""
+    eps = np.asarray(state_errors, dtype=float)
+    eps = np.where(eps > 0.0, eps, 0.0)
+    return np.minimum(1.0, 2.0 * eps + eps * eps)
+
+
 @dataclass(frozen=True)
 class PropagationStats:
     accepted_steps: int

@@ -188,3 +188,12 @@ def test_production_terms_error_texts():
         p.production_terms(0.0, 0.05, nuclei=(n0, n0), radicals=("FAD", "FAD"))
     with pytest.raises(ValueError, match="belong to FAD or TrpH"):
         p.production_terms(0.0, 0.05, nuclei=(n0, n1), radicals=("FAD", "Flavin"))
+
+
+def test_population_bounds_match_the_scalar_rule():
+    from rpm_b200.engine import population_bounds, state_error_to_population_bound
+
+    rng = np.random.default_rng(3)
+    se = np.concatenate([rng.uniform(-1e-3, 1e-3, 2000), rng.uniform(0.0, 2.0, 200), [0.0, -0.0, 1e-300, np.inf]])
+    want = np.array([state_error_to_population_bound(v) for v in se])
+    np.testing.assert_array_equal(population_bounds(se.reshape(-1, 4)), want.reshape(-1, 4))
