@@ -709,7 +709,7 @@ def main() -> None:
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--lanczos", choices=("persistent", "passes"), default="persistent",
                    help="Lanczos iterations of a Krylov step: one persistent launch, or two pass launches each")
-    p.add_argument("--wavefront", type=int, default=0, help="persistent kernel: vectors per wavefront group (0: 12)")
+    p.add_argument("--wavefront", type=int, default=0, help="persistent kernel: vectors per wavefront group (0: equal groups of at most 16)")
     p.add_argument("--parts", type=int, default=1,
                    help="run the step's trajectories as this many concurrent batches on their own streams")
     p.add_argument("--reserve-sms", type=int, default=16,

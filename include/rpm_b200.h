@@ -279,7 +279,8 @@ typedef struct rpm_batch_config {
                                   one; RPM_LANCZOS_PASSES (1): two pass
                                   launches per Lanczos iteration             */
   int wavefront;               /* persistent kernel: vectors that advance
-                                  together through the iterations (<=0: 12) */
+                                  together through the iterations (<=0:
+                                  equal groups of at most 16) */
   int reorth_policy;           /* RPM_REORTH_NONE (0): three-term recurrence
                                   only; RPM_REORTH_PERIODIC (1): after every
                                   `reorth_period` iterations the next Lanczos

@@ -60,7 +60,8 @@ class BatchedPropagator:
     step in one launch per shape group where the shape has a persistent
     kernel (else the per-iteration passes); "passes" launches the two
     shape-specialised passes per iteration.  ``wavefront``: vectors that move
-    through the iterations together in the persistent kernel (0: 12).
+    through the iterations together in the persistent kernel (0: equal groups
+    of at most 16).
     ``reorth_period`` > 0 reorthogonalises the next Lanczos vector against the
     whole basis after every that many iterations (two classical Gram-Schmidt
     passes in FP64 over the complex64 basis); 0 keeps the plain three-term

@@ -1404,7 +1404,15 @@ static void record_step(rpm_batch* Bh, const BatchDev& B, const Layout& L, cudaS
       P.slot0 = (long long)G.b0 * (m + 1);
       P.m = m;
       P.nb = G.nb;
-      P.gv = Bh->cfg.wavefront > 0 ? Bh->cfg.wavefront : 12;
+      // wavefront groups: the requested size, or equal groups of at most 16
+      // vectors (48 vectors: three of 16, 0.1675 ms per iteration against
+      // 0.1755 ms for four of 12; a partial last group costs more)
+      if (Bh->cfg.wavefront > 0) {
+        P.gv = Bh->cfg.wavefront;
+      } else {
+        const int ngroups = (G.nb + 15) / 16;
+        P.gv = (G.nb + ngroups - 1) / ngroups;
+      }
       P.j0 = j0;
       P.j1 = j1;
       P.views = Bh->views_dev;
