@@ -361,7 +361,7 @@ int rpm_spectrum_mac(long long count, void* acc_dev, const void* x_dev, const vo
 /* Kernel of the batched singlet Gram V^H P_S V (replaces the per-basis
  * projection of ENG:521-529): 0 the CUDA-core kernel, 1 (default) the
  * tensor-core kernel (tcgen05, TF32 split into high and low parts, FP32 sums
- * over 128 rows in tensor memory, FP64 across them) wherever the batch allows
+ * over 32 rows in tensor memory, FP64 across them) wherever the batch allows
  * it (every state dimension a multiple of 8, Krylov dimension <= 63).  Read
  * when a batch's step is set up. */
 int rpm_set_gram_kernel(int kernel);
