@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_b_gram_tc(const __grid_constant
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-  unsigned char* raw = base;                              // [kRawStages][k][half][32] float2
+  unsigned char* raw = base;                              // [kRawStages][half][slot][32] float2
   unsigned char* tiles = base + kRawStages * kRawBytes;   // [kTileStages][hi, lo] operand tiles
   __shared__ __align__(8) unsigned long long raw_full[kRawStages], raw_empty[kRawStages], tile_full[kTileStages],
       tile_empty[kTileStages], acc_full[2], acc_empty[2], mma_done;
