@@ -197,3 +197,22 @@ def test_population_bounds_match_the_scalar_rule():
     se = np.concatenate([rng.uniform(-1e-3, 1e-3, 2000), rng.uniform(0.0, 2.0, 200), [0.0, -0.0, 1e-300, np.inf]])
     want = np.array([state_error_to_population_bound(v) for v in se])
     np.testing.assert_array_equal(population_bounds(se.reshape(-1, 4)), want.reshape(-1, 4))
+
+
+def test_oracle_linear_algebra_rejects_bad_sizes_before_any_launch():
+    import ctypes
+
+    size = ctypes.c_longlong()
+    _lib.call("rpm_he_eigh_workspace", 576, 3, ctypes.byref(size))
+    n, nn = 576, 576 * 576
+    assert size.value >= 3 * (5 * n * 8 + 8 + nn * 24)
+    for bad in ((1, 1), (2000, 1), (8, 0)):
+        with pytest.raises(ValueError):
+            _lib.call("rpm_he_eigh_workspace", bad[0], bad[1], ctypes.byref(size))
+    null = ctypes.c_void_p()
+    with pytest.raises(ValueError):  # not a power of two
+        _lib.call("rpm_fft_pow2", 6, 1, null, null, 0, null)
+    with pytest.raises(ValueError):
+        _lib.call("rpm_zgemm_hn", 0, 1, null, null, null, null)
+    with pytest.raises(ValueError):
+        _lib.call("rpm_spectrum_mac", ctypes.c_longlong(0), null, null, null, null)
